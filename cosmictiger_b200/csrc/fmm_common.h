@@ -1,0 +1,112 @@
+// Shared scaffolding for the generated FMM operator headers (fmm_p*.h):
+// host/device qualifiers and type-generic fused multiply-add / sqrt.
+#pragma once
+#include <cmath>
+
+#ifndef CT_HD
+#ifdef __CUDACC__
+#define CT_HD __host__ __device__ __forceinline__
+#else
+#define CT_HD inline
+#endif
+#endif
+
+#ifdef __CUDACC__
+#define CT_HD_FN __host__ __device__ inline
+#else
+#define CT_HD_FN inline
+#endif
+
+CT_HD_FN float ct_fma(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+	return __fmaf_rn(a, b, c);
+#else
+	return std::fma(a, b, c);
+#endif
+}
+CT_HD_FN double ct_fma(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+	return __fma_rn(a, b, c);
+#else
+	return std::fma(a, b, c);
+#endif
+}
+CT_HD_FN float ct_sqrt(float a) {
+#ifdef __CUDA_ARCH__
+	return __fsqrt_rn(a);
+#else
+	return std::sqrt(a);
+#endif
+}
+CT_HD_FN double ct_sqrt(double a) {
+#ifdef __CUDA_ARCH__
+	return __dsqrt_rn(a);
+#else
+	return std::sqrt(a);
+#endif
+}
+
+// Ewald sum sizes: real-space images with distance from the unit cell below 2.6 box
+// lengths, and Fourier vectors with 0 < |h|^2 <= 8 (cosmictiger/ewald_indices.hpp:28-29).
+#define CT_EWALD_NREAL 178
+#define CT_EWALD_NFOUR 92
+
+CT_HD_FN float ct_exp_f(float a) {
+	return expf(a);
+}
+CT_HD_FN double ct_exp_f(double a) {
+	return exp(a);
+}
+template<class T>
+CT_HD_FN void ct_sincos(T a, T* s, T* c) {
+#ifdef __CUDA_ARCH__
+	sincos(a, s, c);
+#else
+	*s = std::sin(a);
+	*c = std::cos(a);
+#endif
+}
+
+// exp(x) from its Taylor series through x^16 (used for small |x| near the origin of the
+// Ewald sum, cosmictiger/math.hpp:169-206).
+template<class T>
+CT_HD_FN T ct_exp_series(T x) {
+	// 1/k!, k = 16..0
+	const double c[17] = { 4.7794773323873853e-14, 7.6471637318198164e-13, 1.1470745597729725e-11, 1.6059043836821613e-10, 2.08767569878681e-09,
+			2.505210838544172e-08, 2.7557319223985888e-07, 2.7557319223985893e-06, 2.4801587301587302e-05, 0.00019841269841269841,
+			0.0013888888888888889, 0.0083333333333333332, 0.041666666666666664, 0.16666666666666666, 0.5, 1.0, 1.0 };
+	T w = T(c[0]);
+	for (int i = 1; i < 17; i++) {
+		w = ct_fma(w, x, T(c[i]));
+	}
+	return w;
+}
+
+// erf(x) from its Taylor series 2/sqrt(pi) sum_n (-1)^n x^(2n+1) / (n! (2n+1)), n = 0..14
+// (cosmictiger/math.hpp:160-167).
+template<class T>
+CT_HD_FN T ct_erf_series(T x) {
+	const double c[15] = { 1.1283791670955126, -0.37612638903183754, 0.11283791670955126, -0.026866170645131252, 0.0052239776254421878,
+			-0.00085483270234508528, 0.00012055332981789664, -1.4925650358406251e-05, 1.6462114365889247e-06, -1.6365844691234924e-07,
+			1.4807192815879218e-08, -1.2290555301717926e-09, 9.4227590646504108e-11, -6.7113668551641104e-12, 4.4632242632864774e-13 };
+	const T x2 = x * x;
+	T w = T(c[14]);
+	for (int i = 13; i >= 0; i--) {
+		w = ct_fma(w, x2, T(c[i]));
+	}
+	return w * x;
+}
+
+// erfc(x) and exp(-x^2) by Abramowitz & Stegun 7.1.26 (|error| <= 1.5e-7), the form the
+// reference uses on the device (cosmictiger/math.hpp:56-71).
+template<class T>
+CT_HD_FN void ct_erfcexp(T x, T* ec, T* ex) {
+	const T p = T(0.3275911), a1 = T(0.254829592), a2 = T(-0.284496736), a3 = T(1.421413741), a4 = T(-1.453152027), a5 = T(1.061405429);
+	const T t = T(1) / ct_fma(p, x, T(1));
+	*ex = ct_exp_f(-x * x);
+	T s = ct_fma(a5, t, a4);
+	s = ct_fma(s, t, a3);
+	s = ct_fma(s, t, a2);
+	s = ct_fma(s, t, a1);
+	*ec = s * t * *ex;
+}

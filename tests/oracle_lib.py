@@ -1,0 +1,153 @@
+"""ctypes bindings of the CPU oracle (oracle/libct_oracle.so): test infrastructure only.
+
+Imported by the tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg, always
+as the checker of the CUDA path, never as the thing measured or shipped.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+LIB = os.path.join(ORACLE_DIR, "libct_oracle.so")
+
+NODE_DTYPE = np.dtype(
+    [
+        ("key", np.uint64),
+        ("part_begin", np.int32),
+        ("part_end", np.int32),
+        ("child_left", np.int32),
+        ("child_right", np.int32),
+        ("pos", np.uint32, 3),
+        ("radius", np.float32),
+        ("box_begin", np.int32, 3),
+        ("box_end", np.int32, 3),
+        ("leaf", np.int32),
+        ("depth", np.int32),
+        ("multi", np.float32, 37),
+    ],
+    align=True,
+)
+
+
+class KickParams(ctypes.Structure):
+    _fields_ = [
+        ("sign", ctypes.c_float),
+        ("min_rung", ctypes.c_int),
+        ("a", ctypes.c_float),
+        ("t0", ctypes.c_float),
+        ("theta", ctypes.c_float),
+        ("h", ctypes.c_float),
+        ("eta", ctypes.c_float),
+        ("GM", ctypes.c_float),
+        ("max_dt", ctypes.c_float),
+        ("save_force", ctypes.c_int),
+        ("first_call", ctypes.c_int),
+        ("ascending", ctypes.c_int),
+        ("descending", ctypes.c_int),
+        ("top", ctypes.c_int),
+        ("do_phi", ctypes.c_int),
+    ]
+
+
+class KickReturn(ctypes.Structure):
+    _fields_ = [
+        ("max_rung", ctypes.c_int),
+        ("pot", ctypes.c_double),
+        ("kin", ctypes.c_double),
+        ("dkin", ctypes.c_double),
+        ("xmom", ctypes.c_double),
+        ("ymom", ctypes.c_double),
+        ("zmom", ctypes.c_double),
+        ("nmom", ctypes.c_double),
+    ]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(ORACLE_DIR, f) for f in ("ct_oracle.cpp", "ct_oracle.h")]
+    csrc = os.path.join(ROOT, "cosmictiger_b200", "csrc")
+    deps += [os.path.join(csrc, f) for f in ("fmm_p7.h", "fmm_p5.h", "fmm_common.h")]
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+class Oracle:
+    def __init__(self, path):
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        L.ct_or_tree_build.restype = ctypes.c_int
+        L.ct_or_kick.restype = ctypes.c_int
+        L.ct_or_sort_by_rung.restype = ctypes.c_int
+        for name in ("ct_or_greens", "ct_or_ewald_greens", "ct_or_ewald_greens_d"):
+            getattr(L, name).restype = ctypes.c_int
+
+    # ---- operators
+    def op(self, name, order, *arrays, flag=None):
+        args = [ctypes.c_int(order)] + [_p(a) for a in arrays]
+        if flag is not None:
+            args.append(ctypes.c_int(flag))
+        return getattr(self.lib, "ct_or_" + name)(*args)
+
+    # ---- tree
+    def tree_build(self, x, y, z, v, rung, theta, hsoft, bucket=128, order=7, begin=0):
+        n = len(x)
+        max_nodes = max(64, 8 * n // max(bucket // 4, 1) + 1024)
+        while True:
+            nodes = np.zeros(max_nodes, NODE_DTYPE)
+            cnt = self.lib.ct_or_tree_build(
+                ctypes.c_int(order), ctypes.c_int(n), ctypes.c_int(begin), _p(x), _p(y), _p(z), _p(v), _p(rung),
+                ctypes.c_double(theta), ctypes.c_double(hsoft), ctypes.c_int(bucket), _p(nodes), ctypes.c_int(max_nodes))
+            if cnt >= 0:
+                return nodes[:cnt]
+            max_nodes *= 2
+            if max_nodes > 1 << 28:
+                raise RuntimeError("oracle tree build failed")
+
+    def kick(self, params, nodes, x, y, z, v, rung, order=7, nthreads=0, save_force=True):
+        n = len(x)
+        gx = np.zeros(n, np.float32) if save_force else None
+        gy = np.zeros(n, np.float32) if save_force else None
+        gz = np.zeros(n, np.float32) if save_force else None
+        pot = np.zeros(n, np.float32) if save_force else None
+        rc = KickReturn()
+        flops = ctypes.c_double(0)
+        err = self.lib.ct_or_kick(ctypes.c_int(order), ctypes.byref(params), ctypes.c_int(len(nodes)), _p(nodes), _p(x), _p(y), _p(z), _p(v),
+                                  _p(rung), _p(gx), _p(gy), _p(gz), _p(pot), ctypes.byref(rc), ctypes.c_int(nthreads), ctypes.byref(flops))
+        if err:
+            raise RuntimeError("oracle kick error %d" % err)
+        return (gx, gy, gz, pot), rc, flops.value
+
+    def drift(self, x, y, z, v, rung, which_rung, a, dt, drag=0.0):
+        self.lib.ct_or_drift(ctypes.c_int(len(x)), _p(x), _p(y), _p(z), _p(v), _p(rung), ctypes.c_int(which_rung), ctypes.c_float(a),
+                             ctypes.c_float(dt), ctypes.c_double(drag))
+
+    def sort_by_rung(self, x, y, z, v, rung, minrung, begin=0):
+        return self.lib.ct_or_sort_by_rung(ctypes.c_int(len(x)), ctypes.c_int(begin), ctypes.c_int(minrung), _p(x), _p(y), _p(z), _p(v), _p(rung))
+
+    def direct_ewald(self, x, y, z, sx, sy, sz, h, nthreads=0):
+        ns = len(sx)
+        out = [np.zeros(ns) for _ in range(4)]
+        self.lib.ct_or_direct_ewald(ctypes.c_int(len(x)), _p(x), _p(y), _p(z), ctypes.c_int(ns), _p(sx), _p(sy), _p(sz), ctypes.c_double(h),
+                                    *[_p(a) for a in out], ctypes.c_int(nthreads))
+        return out
+
+
+_cached = None
+
+
+def load(build=True):
+    global _cached
+    if _cached is not None:
+        return _cached
+    if build and _stale():
+        subprocess.check_call(["make", "-s", "-C", ORACLE_DIR, "libct_oracle.so"])
+    _cached = Oracle(LIB)
+    return _cached
