@@ -1,0 +1,259 @@
+"""B200-native gravity step of CosmicTiger: tree build, kick, drift behind a C ABI.
+
+The compute path is libct_gravity.so (hand-written sm_100a CUDA, include/ct_gravity.h).  This
+module is the host-side mirror of the reference's call surface for that path:
+
+    reference (dmarce1/cosmictiger)                      here
+    particles_sort_by_rung(minrung)  particles.cpp:1029   Box.sort_by_rung(minrung)
+    tree_create(tree_create_params)  tree.cpp:273         Box.tree_create(theta, hsoft, bucket, min_rung)
+    kick(kick_params, L, pos, root, {root}, {root})       Box.kick(KickParams) -> KickReturn
+                                     kick.cpp:150
+    drift(scale, dt, ..., rung)      drift.cpp:33         Box.drift(rung, a, dt, drag)
+
+There is no CPU fallback: importing works without a GPU, but creating a Context requires the
+built library and a CUDA device and raises otherwise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libct_gravity.so")
+
+CT_OK = 0
+_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory / HBM budget", -4: "capacity exceeded", -5: "call out of order"}
+
+
+class GravityError(RuntimeError):
+    pass
+
+
+class KickParams(ctypes.Structure):
+    """Mirror of kick_params (cosmictiger/kick.hpp:138-186)."""
+
+    _fields_ = [
+        ("sign", ctypes.c_float),
+        ("min_rung", ctypes.c_int),
+        ("a", ctypes.c_float),
+        ("t0", ctypes.c_float),
+        ("theta", ctypes.c_float),
+        ("h", ctypes.c_float),
+        ("eta", ctypes.c_float),
+        ("GM", ctypes.c_float),
+        ("max_dt", ctypes.c_float),
+        ("save_force", ctypes.c_int),
+        ("first_call", ctypes.c_int),
+        ("ascending", ctypes.c_int),
+        ("descending", ctypes.c_int),
+        ("top", ctypes.c_int),
+        ("do_phi", ctypes.c_int),
+    ]
+
+    @classmethod
+    def make(cls, theta, h, GM, eta, min_rung=0, a=1.0, t0=1.0, max_dt=1e30, save_force=True, first_call=True, ascending=True,
+             descending=True, top=True, do_phi=True, sign=1.0):
+        return cls(sign=sign, min_rung=min_rung, a=a, t0=t0, theta=theta, h=h, eta=eta, GM=GM, max_dt=max_dt, save_force=int(save_force),
+                   first_call=int(first_call), ascending=int(ascending), descending=int(descending), top=int(top), do_phi=int(do_phi))
+
+
+class KickReturn(ctypes.Structure):
+    """Mirror of kick_return (cosmictiger/kick.hpp:92-136)."""
+
+    _fields_ = [
+        ("max_rung", ctypes.c_int),
+        ("pot", ctypes.c_double),
+        ("kin", ctypes.c_double),
+        ("dkin", ctypes.c_double),
+        ("xmom", ctypes.c_double),
+        ("ymom", ctypes.c_double),
+        ("zmom", ctypes.c_double),
+        ("nmom", ctypes.c_double),
+    ]
+
+
+class TreeParams(ctypes.Structure):
+    _fields_ = [("min_rung", ctypes.c_int), ("theta", ctypes.c_double), ("hsoft", ctypes.c_double), ("bucket", ctypes.c_int)]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "pp_pairs", "cc_direct", "cc_ewald", "cp_pairs", "pc_pairs", "nodes", "leaves", "flops", "flops_pp", "flops_cc",
+        "ms_tree", "ms_walk", "ms_m2l", "ms_l2l", "ms_leaf", "ms_drift")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+NODE_DTYPE = np.dtype(
+    [
+        ("key", np.uint64),
+        ("part_begin", np.int32),
+        ("part_end", np.int32),
+        ("child_left", np.int32),
+        ("child_right", np.int32),
+        ("pos", np.uint32, 3),
+        ("radius", np.float32),
+        ("box_begin", np.int32, 3),
+        ("box_end", np.int32, 3),
+        ("leaf", np.int32),
+        ("depth", np.int32),
+        ("multi", np.float32, 37),
+    ],
+    align=True,
+)
+
+_lib = None
+
+
+def library():
+    """Load libct_gravity.so; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise GravityError("libct_gravity.so is not built (run __graft_entry__.build() or python cosmictiger_b200/build.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i64, i32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int
+    L.ct_ctx_create.argtypes = [ctypes.POINTER(vp), i32, ctypes.c_size_t, i32]
+    L.ct_ctx_destroy.argtypes = [vp]
+    L.ct_ctx_destroy.restype = None
+    L.ct_last_error.argtypes = [vp]
+    L.ct_last_error.restype = ctypes.c_char_p
+    L.ct_box_create.argtypes = [vp, i64, ctypes.POINTER(i32)]
+    L.ct_box_destroy.argtypes = [vp, i32]
+    L.ct_box_size.argtypes = [vp, i32]
+    L.ct_box_size.restype = i64
+    L.ct_box_upload.argtypes = [vp, i32, vp, vp, vp, vp, vp]
+    L.ct_box_upload_device.argtypes = [vp, i32, vp, vp, vp, vp, vp]
+    L.ct_box_download.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.ct_box_download_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.ct_sort_by_rung.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
+    L.ct_tree_create.argtypes = [vp, i32, ctypes.POINTER(TreeParams), ctypes.POINTER(i64)]
+    L.ct_kick.argtypes = [vp, i32, ctypes.POINTER(KickParams), ctypes.POINTER(KickReturn)]
+    L.ct_drift.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_double]
+    L.ct_tree_download.argtypes = [vp, i32, vp, i64, ctypes.POINTER(i64)]
+    L.ct_get_counters.argtypes = [vp, i32, ctypes.POINTER(Counters)]
+    L.ct_synchronize.argtypes = [vp]
+    L.ct_direct_ewald.argtypes = [vp, i32, i64, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else int(a))
+
+
+class Context:
+    """One device, one stream, device-resident boxes (ct_ctx_create)."""
+
+    def __init__(self, device=0, hbm_budget=0, order=7):
+        self.lib = library()
+        h = ctypes.c_void_p()
+        rc = self.lib.ct_ctx_create(ctypes.byref(h), device, hbm_budget, order)
+        if rc != CT_OK:
+            raise GravityError("ct_ctx_create failed (%s)" % _ERRORS.get(rc, rc))
+        self.h = h
+        self.order = order
+
+    def check(self, rc, what):
+        if rc != CT_OK:
+            raise GravityError("%s: %s (%s)" % (what, self.lib.ct_last_error(self.h).decode(), _ERRORS.get(rc, rc)))
+
+    def box(self, n):
+        return Box(self, n)
+
+    def synchronize(self):
+        self.check(self.lib.ct_synchronize(self.h), "ct_synchronize")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ct_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Box:
+    """A periodic unit box of particles with its tree, resident on the device."""
+
+    def __init__(self, ctx, n):
+        self.ctx = ctx
+        self.n = int(n)
+        bid = ctypes.c_int()
+        ctx.check(ctx.lib.ct_box_create(ctx.h, self.n, ctypes.byref(bid)), "ct_box_create")
+        self.id = bid.value
+        self.tree_params = None
+
+    def upload(self, x, y, z, vxyz, rung):
+        """Host arrays: x,y,z uint32 fixed32; vxyz float32 (n,3); rung int8."""
+        arrs = [np.ascontiguousarray(x, np.uint32), np.ascontiguousarray(y, np.uint32), np.ascontiguousarray(z, np.uint32),
+                np.ascontiguousarray(vxyz, np.float32), np.ascontiguousarray(rung, np.int8)]
+        for a in arrs[:3] + [arrs[4]]:
+            if a.shape[0] != self.n:
+                raise ValueError("array length differs from the box size")
+        self.ctx.check(self.ctx.lib.ct_box_upload(self.ctx.h, self.id, *[_p(a) for a in arrs]), "ct_box_upload")
+
+    def upload_device(self, x, y, z, vxyz, rung):
+        """Device pointers (e.g. torch tensor data_ptr()) with the same layout."""
+        self.ctx.check(self.ctx.lib.ct_box_upload_device(self.ctx.h, self.id, *[_p(a) for a in (x, y, z, vxyz, rung)]), "ct_box_upload_device")
+
+    def download(self, forces=False):
+        n = self.n
+        x, y, z = (np.empty(n, np.uint32) for _ in range(3))
+        v = np.empty((n, 3), np.float32)
+        r = np.empty(n, np.int8)
+        g = [np.empty(n, np.float32) for _ in range(4)] if forces else [None] * 4
+        self.ctx.check(self.ctx.lib.ct_box_download(self.ctx.h, self.id, _p(x), _p(y), _p(z), _p(v), _p(r), *[_p(a) for a in g]), "ct_box_download")
+        out = {"x": x, "y": y, "z": z, "v": v, "rung": r}
+        if forces:
+            out.update(gx=g[0], gy=g[1], gz=g[2], pot=g[3])
+        return out
+
+    def sort_by_rung(self, min_rung):
+        rb = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.ct_sort_by_rung(self.ctx.h, self.id, min_rung, ctypes.byref(rb)), "ct_sort_by_rung")
+        return rb.value
+
+    def tree_create(self, theta, hsoft, bucket=128, min_rung=0):
+        p = TreeParams(min_rung=min_rung, theta=theta, hsoft=hsoft, bucket=bucket)
+        cnt = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.ct_tree_create(self.ctx.h, self.id, ctypes.byref(p), ctypes.byref(cnt)), "ct_tree_create")
+        self.tree_params = p
+        return cnt.value
+
+    def kick(self, params):
+        rc = KickReturn()
+        self.ctx.check(self.ctx.lib.ct_kick(self.ctx.h, self.id, ctypes.byref(params), ctypes.byref(rc)), "ct_kick")
+        return rc
+
+    def drift(self, rung, a, dt, drag=0.0):
+        self.ctx.check(self.ctx.lib.ct_drift(self.ctx.h, self.id, rung, a, dt, drag), "ct_drift")
+
+    def tree(self):
+        cnt = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.ct_tree_download(self.ctx.h, self.id, None, 0, ctypes.byref(cnt)), "ct_tree_download")
+        nodes = np.zeros(cnt.value, NODE_DTYPE)
+        self.ctx.check(self.ctx.lib.ct_tree_download(self.ctx.h, self.id, _p(nodes), cnt.value, ctypes.byref(cnt)), "ct_tree_download")
+        return nodes
+
+    def counters(self):
+        c = Counters()
+        self.ctx.check(self.ctx.lib.ct_get_counters(self.ctx.h, self.id, ctypes.byref(c)), "ct_get_counters")
+        return c.as_dict()
+
+    def direct_ewald(self, sx, sy, sz, h):
+        ns = len(sx)
+        out = [np.empty(ns) for _ in range(4)]
+        sx, sy, sz = (np.ascontiguousarray(a, np.uint32) for a in (sx, sy, sz))
+        self.ctx.check(self.ctx.lib.ct_direct_ewald(self.ctx.h, self.id, ns, _p(sx), _p(sy), _p(sz), h, *[_p(a) for a in out]), "ct_direct_ewald")
+        return out
+
+    def close(self):
+        if self.ctx is not None and self.ctx.h is not None and self.id is not None:
+            self.ctx.lib.ct_box_destroy(self.ctx.h, self.id)
+            self.id = None

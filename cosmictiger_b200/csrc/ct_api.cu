@@ -1,0 +1,871 @@
+// C ABI of the gravity step: contexts, boxes, transfers, drift, rung sort, direct Ewald.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "ct_internal.cuh"
+#include "fmm_p7.h"
+
+namespace ct {
+
+ct_status fail(Ctx* c, ct_status code, const std::string& msg) {
+	if (c) {
+		c->err = msg;
+	}
+	return code;
+}
+
+ct_status cuda_check(Ctx* c, cudaError_t e, const char* what) {
+	return fail(c, e == cudaErrorMemoryAllocation ? CT_ERR_MEMORY : CT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+ct_status dalloc(Ctx* c, void** p, size_t bytes, const char* what) {
+	*p = nullptr;
+	if (bytes == 0) {
+		bytes = 16;
+	}
+	if (c->budget && c->used + bytes > c->budget) {
+		return fail(c, CT_ERR_MEMORY, std::string("HBM budget exhausted allocating ") + what);
+	}
+	const cudaError_t e = cudaMalloc(p, bytes);
+	if (e != cudaSuccess) {
+		cudaGetLastError();
+		return fail(c, CT_ERR_MEMORY, std::string("cudaMalloc failed for ") + what + ": " + cudaGetErrorString(e));
+	}
+	c->used += bytes;
+	return CT_OK;
+}
+
+void dfree(Ctx* c, void* p, size_t bytes) {
+	if (p) {
+		cudaFree(p);
+		c->used -= std::min(c->used, bytes == 0 ? size_t(16) : bytes);
+	}
+}
+
+void* scratch(Ctx* c, int slot, size_t bytes, ct_status* st) {
+	if ((int) c->scratch.size() <= slot) {
+		c->scratch.resize(slot + 1);
+	}
+	DevBuf& b = c->scratch[slot];
+	if (b.bytes < bytes || !b.p) {
+		if (b.p) {
+			cudaStreamSynchronize(c->stream);
+			dfree(c, b.p, b.bytes);
+			b.p = nullptr;
+			b.bytes = 0;
+		}
+		const size_t want = std::max(bytes + bytes / 4, (size_t) 4096);
+		const ct_status s = dalloc(c, &b.p, want, "scratch");
+		if (s != CT_OK) {
+			*st = s;
+			return nullptr;
+		}
+		b.bytes = want;
+	}
+	return b.p;
+}
+
+namespace {
+
+Box* get_box(Ctx* c, int id) {
+	if (!c || id < 0 || id >= (int) c->boxes.size()) {
+		return nullptr;
+	}
+	return c->boxes[id];
+}
+
+int grid(Ctx* c, int64_t n, int tpb) {
+	return (int) std::max<int64_t>(1, std::min<int64_t>((n + tpb - 1) / tpb, (int64_t) c->nsm * 8));
+}
+
+__global__ void k_aos_to_soa(int64_t n, const float* __restrict__ vxyz, float* v0, float* v1, float* v2) {
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+		v0[i] = vxyz[3 * i];
+		v1[i] = vxyz[3 * i + 1];
+		v2[i] = vxyz[3 * i + 2];
+	}
+}
+
+__global__ void k_soa_to_aos(int64_t n, const float* v0, const float* v1, const float* v2, float* __restrict__ vxyz) {
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+		vxyz[3 * i] = v0[i];
+		vxyz[3 * i + 1] = v1[i];
+		vxyz[3 * i + 2] = v2[i];
+	}
+}
+
+// Drift of one rung (src/drift.cu:36-154; lightcone capture excluded): FP64 position update,
+// periodic wrap, truncating fixed32 store.  Particles of other rungs are not touched.
+__global__ void __launch_bounds__(256) k_drift(int64_t b, int64_t n, uint32_t* __restrict__ x0, uint32_t* __restrict__ x1, uint32_t* __restrict__ x2,
+		float* __restrict__ v0, float* __restrict__ v1, float* __restrict__ v2, const int8_t* __restrict__ rung, int which, double c1, double drag_c0,
+		int do_drag) {
+	for (int64_t i = b + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+		if (rung[i] != which) {
+			continue;
+		}
+		uint32_t* X[3] = { x0, x1, x2 };
+		float* V[3] = { v0, v1, v2 };
+#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			const double xo = fixed_to_double(X[d][i]);
+			double x1d = __dadd_rn(xo, __dmul_rn((double) V[d][i], c1));
+			x1d = __dsub_rn(x1d, (double) (x1d >= 1.0));
+			x1d = __dadd_rn(x1d, (double) (x1d < 0.0));
+			X[d][i] = fixed_from_double(x1d);
+		}
+		if (do_drag) {
+#pragma unroll
+			for (int d = 0; d < 3; d++) {
+				V[d][i] = (float) ((double) V[d][i] * drag_c0);
+			}
+		}
+	}
+}
+
+// ---- rung partition (src/particles.cpp:1029-1076): same exact permutation rule as the tree
+// partition, with predicate rung < minrung on the left.
+__global__ void k_rung_flags(int64_t b, int64_t e, const int8_t* rung, int minrung, int* lt) {
+	for (int64_t i = b + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < e; i += (int64_t) gridDim.x * blockDim.x) {
+		lt[i - b] = rung[i] < minrung;
+	}
+}
+__global__ void k_rung_mis(int64_t b, int64_t e, const int* lt, const int* m, int* misL, int* misR) {
+	const int64_t s = b + *m;
+	for (int64_t i = b + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < e; i += (int64_t) gridDim.x * blockDim.x) {
+		const int f = lt[i - b];
+		misL[i - b] = (i < s) && !f;
+		misR[i - b] = (i >= s) && f;
+	}
+}
+__global__ void k_rung_pos(int64_t b, int64_t e, const int* misL, const int* misR, const int* exL, const int* exR, const int* totR, int* posL,
+		int* posR) {
+	for (int64_t i = b + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < e; i += (int64_t) gridDim.x * blockDim.x) {
+		const int64_t k = i - b;
+		if (misL[k]) {
+			posL[exL[k]] = (int) i;
+		}
+		if (misR[k]) {
+			posR[*totR - 1 - exR[k]] = (int) i;
+		}
+	}
+}
+__global__ void k_rung_swap(const int* posL, const int* posR, const int* nmis, uint32_t* x0, uint32_t* x1, uint32_t* x2, float* v0, float* v1,
+		float* v2, int8_t* rung) {
+	const int n = *nmis;
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		const int a = posL[k], c = posR[k];
+		uint32_t t = x0[a];
+		x0[a] = x0[c];
+		x0[c] = t;
+		t = x1[a];
+		x1[a] = x1[c];
+		x1[c] = t;
+		t = x2[a];
+		x2[a] = x2[c];
+		x2[c] = t;
+		float f = v0[a];
+		v0[a] = v0[c];
+		v0[c] = f;
+		f = v1[a];
+		v1[a] = v1[c];
+		v1[c] = f;
+		f = v2[a];
+		v2[a] = v2[c];
+		v2[c] = f;
+		const int8_t r = rung[a];
+		rung[a] = rung[c];
+		rung[c] = r;
+	}
+}
+
+// ---- FP64 direct Ewald (accuracy reference)
+__global__ void k_struct_factor(int64_t n, const uint32_t* x0, const uint32_t* x1, const uint32_t* x2, const float* four, double* CS) {
+	const int h = blockIdx.y;
+	const double hx = four[3 * h], hy = four[3 * h + 1], hz = four[3 * h + 2];
+	double c = 0.0, s = 0.0;
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+		const double ph = 6.283185307179586 * (hx * fixed_to_double(x0[i]) + hy * fixed_to_double(x1[i]) + hz * fixed_to_double(x2[i]));
+		double sn, cs;
+		sincos(ph, &sn, &cs);
+		c += cs;
+		s += sn;
+	}
+	for (int o = 16; o; o >>= 1) {
+		c += __shfl_xor_sync(0xffffffffu, c, o);
+		s += __shfl_xor_sync(0xffffffffu, s, o);
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicAdd(CS + 2 * h, c);
+		atomicAdd(CS + 2 * h + 1, s);
+	}
+}
+
+__device__ void ewald_pair_fp64(double dx, double dy, double dz, const float* real, double& phi, double* g) {
+	const double alpha = 2.0, tsp = 1.1283791670955126;
+	const double r2 = dx * dx + dy * dy + dz * dz;
+	const double r = sqrt(r2);
+	if (alpha * r < 0.05) {
+		const double a2r2 = alpha * alpha * r2;
+		phi += tsp * alpha * (1.0 - a2r2 / 3.0 + a2r2 * a2r2 / 10.0 - a2r2 * a2r2 * a2r2 / 42.0 + a2r2 * a2r2 * a2r2 * a2r2 / 216.0);
+		const double c = tsp * alpha * alpha * alpha * (-2.0 / 3.0 + 0.4 * a2r2 - a2r2 * a2r2 / 7.0 + a2r2 * a2r2 * a2r2 / 27.0);
+		g[0] += c * dx;
+		g[1] += c * dy;
+		g[2] += c * dz;
+	} else {
+		const double e = erf(alpha * r);
+		phi += e / r;
+		const double dp = (-e / r2 + tsp * alpha * exp(-alpha * alpha * r2) / r) / r;
+		g[0] += dp * dx;
+		g[1] += dp * dy;
+		g[2] += dp * dz;
+	}
+	for (int i = 0; i < CT_EWALD_NREAL; i++) {
+		const double x = dx - real[3 * i], y = dy - real[3 * i + 1], z = dz - real[3 * i + 2];
+		const double s2 = x * x + y * y + z * z;
+		if (s2 < 2.6 * 2.6) {
+			const double s = sqrt(s2);
+			const double ec = erfc(alpha * s);
+			phi -= ec / s;
+			const double dp = (ec / s2 + tsp * alpha * exp(-alpha * alpha * s2) / s) / s;
+			g[0] += dp * x;
+			g[1] += dp * y;
+			g[2] += dp * z;
+		}
+	}
+	phi += 3.141592653589793 / (alpha * alpha);
+}
+
+__global__ void __launch_bounds__(256) k_direct_ewald(int64_t n, const uint32_t* x0, const uint32_t* x1, const uint32_t* x2, const uint32_t* sx,
+		const uint32_t* sy, const uint32_t* sz, double h, const float* real, double* out) {
+	__shared__ double red[8][4];
+	__shared__ float sreal[3 * CT_EWALD_NREAL];
+	for (int i = threadIdx.x; i < 3 * CT_EWALD_NREAL; i += blockDim.x) {
+		sreal[i] = real[i];
+	}
+	__syncthreads();
+	const int s = blockIdx.x;
+	const uint32_t X = sx[s], Y = sy[s], Z = sz[s];
+	const double hinv = 1.0 / h, h2inv = hinv * hinv, h3inv = h2inv * hinv;
+	double phi = 0.0, g[3] = { 0.0, 0.0, 0.0 };
+	for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+		const double dx = (double) (int32_t) (X - x0[j]) * (1.0 / 4294967296.0);
+		const double dy = (double) (int32_t) (Y - x1[j]) * (1.0 / 4294967296.0);
+		const double dz = (double) (int32_t) (Z - x2[j]) * (1.0 / 4294967296.0);
+		const double r2 = dx * dx + dy * dy + dz * dz;
+		if (r2 > h * h) {
+			const double rinv = 1.0 / sqrt(r2);
+			const double r3 = rinv * rinv * rinv;
+			g[0] -= dx * r3;
+			g[1] -= dy * r3;
+			g[2] -= dz * r3;
+			phi -= rinv;
+		} else {
+			const double q2 = r2 * h2inv;
+			double f = 315. / 128.;
+			f = fma(f, q2, -385. / 32.);
+			f = fma(f, q2, 1485. / 64.);
+			f = fma(f, q2, -693. / 32.);
+			f = fma(f, q2, 1155. / 128.);
+			f *= h3inv;
+			double p = -63. / 256.;
+			p = fma(p, q2, 385. / 256.);
+			p = fma(p, q2, -495. / 128.);
+			p = fma(p, q2, 693. / 128.);
+			p = fma(p, q2, -1155. / 256.);
+			p = fma(p, q2, 693. / 256.);
+			p *= hinv;
+			g[0] -= dx * f;
+			g[1] -= dy * f;
+			g[2] -= dz * f;
+			phi -= p;
+		}
+		double pc = 0.0, gc[3] = { 0.0, 0.0, 0.0 };
+		ewald_pair_fp64(dx, dy, dz, sreal, pc, gc);
+		phi += pc;
+		g[0] -= gc[0];
+		g[1] -= gc[1];
+		g[2] -= gc[2];
+	}
+	double v[4] = { g[0], g[1], g[2], phi };
+	for (int k = 0; k < 4; k++) {
+		for (int o = 16; o; o >>= 1) {
+			v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+		}
+	}
+	if ((threadIdx.x & 31) == 0) {
+		for (int k = 0; k < 4; k++) {
+			red[threadIdx.x >> 5][k] = v[k];
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x < 4) {
+		double t = 0.0;
+		for (int w = 0; w < (int) (blockDim.x >> 5); w++) {
+			t += red[w][threadIdx.x];
+		}
+		out[4 * s + threadIdx.x] = t;
+	}
+}
+
+__global__ void k_direct_ewald_four(int nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, const float* four, const double* CS, double h,
+		double* out) {
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= nsink) {
+		return;
+	}
+	const double xi[3] = { fixed_to_double(sx[s]), fixed_to_double(sy[s]), fixed_to_double(sz[s]) };
+	double phi = 693.0 / 256.0 / h;  // the self pair's softened term is excluded (kick.cu:265)
+	double g[3] = { 0, 0, 0 };
+	for (int k = 0; k < CT_EWALD_NFOUR; k++) {
+		const double hx = four[3 * k], hy = four[3 * k + 1], hz = four[3 * k + 2];
+		const double h2 = hx * hx + hy * hy + hz * hz;
+		const double c0 = -exp(-9.869604401089358 * h2 / 4.0) / (3.141592653589793 * h2);
+		double sn, cs;
+		sincos(6.283185307179586 * (hx * xi[0] + hy * xi[1] + hz * xi[2]), &sn, &cs);
+		phi += c0 * (cs * CS[2 * k] + sn * CS[2 * k + 1]);
+		const double sd = sn * CS[2 * k] - cs * CS[2 * k + 1];
+		g[0] += c0 * 6.283185307179586 * hx * sd;
+		g[1] += c0 * 6.283185307179586 * hy * sd;
+		g[2] += c0 * 6.283185307179586 * hz * sd;
+	}
+	out[4 * s] += g[0];
+	out[4 * s + 1] += g[1];
+	out[4 * s + 2] += g[2];
+	out[4 * s + 3] += phi;
+}
+
+}  // namespace
+
+ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag) {
+	const double c1 = (double) dt / (double) a;
+	const double c0 = drag != 0.0 ? 1.0 / (1.0 + drag * (double) dt) : 1.0;
+	const int64_t np = b->n - b->rung_begin;
+	cudaEventRecord(c->ev[6], c->stream);
+	if (np > 0) {
+		k_drift<<<grid(c, np, 256), 256, 0, c->stream>>>(b->rung_begin, b->n, b->x[0], b->x[1], b->x[2], b->v[0], b->v[1], b->v[2], b->rung, rung, c1, c0,
+				drag != 0.0);
+	}
+	cudaEventRecord(c->ev[7], c->stream);
+	CT_CUDA(c, cudaGetLastError());
+	b->tree_valid = false;
+	return CT_OK;
+}
+
+ct_status sort_by_rung_run(Ctx* c, Box* b, int minrung) {
+	cudaStream_t st = c->stream;
+	if (minrung == 0) {
+		b->rung_begin = 0;
+		b->tree_valid = false;
+		return CT_OK;
+	}
+	const int64_t beg = b->rung_begin, e = b->n, n = e - beg;
+	if (n <= 0) {
+		return CT_OK;
+	}
+	ct_status s = CT_OK;
+	int* lt = (int*) scratch(c, 21, sizeof(int) * n, &s);
+	int* misL = (int*) scratch(c, 22, sizeof(int) * n, &s);
+	int* misR = (int*) scratch(c, 23, sizeof(int) * n, &s);
+	int* exL = (int*) scratch(c, 24, sizeof(int) * n, &s);
+	int* exR = (int*) scratch(c, 25, sizeof(int) * n, &s);
+	int* posL = (int*) scratch(c, 26, sizeof(int) * n, &s);
+	int* posR = (int*) scratch(c, 27, sizeof(int) * n, &s);
+	int* tot = (int*) scratch(c, 28, sizeof(int) * 4, &s);
+	CT_TRY(s);
+	size_t need = 0, need2 = 0;
+	cub::DeviceReduce::Sum(nullptr, need, lt, tot, (int) n, st);
+	cub::DeviceScan::ExclusiveSum(nullptr, need2, misL, exL, (int) n, st);
+	void* tmp = scratch(c, 29, std::max(need, need2) + 256, &s);
+	CT_TRY(s);
+	need = std::max(need, need2);
+	k_rung_flags<<<grid(c, n, 256), 256, 0, st>>>(beg, e, b->rung, minrung, lt);
+	CT_CUDA(c, cub::DeviceReduce::Sum(tmp, need, lt, tot, (int) n, st));
+	k_rung_mis<<<grid(c, n, 256), 256, 0, st>>>(beg, e, lt, tot, misL, misR);
+	CT_CUDA(c, cub::DeviceScan::ExclusiveSum(tmp, need, misL, exL, (int) n, st));
+	CT_CUDA(c, cub::DeviceReduce::Sum(tmp, need, misL, tot + 1, (int) n, st));
+	CT_CUDA(c, cub::DeviceScan::ExclusiveSum(tmp, need, misR, exR, (int) n, st));
+	CT_CUDA(c, cub::DeviceReduce::Sum(tmp, need, misR, tot + 2, (int) n, st));
+	k_rung_pos<<<grid(c, n, 256), 256, 0, st>>>(beg, e, misL, misR, exL, exR, tot + 2, posL, posR);
+	k_rung_swap<<<grid(c, n, 256), 256, 0, st>>>(posL, posR, tot + 1, b->x[0], b->x[1], b->x[2], b->v[0], b->v[1], b->v[2], b->rung);
+	int* h = (int*) c->pinned;
+	CT_CUDA(c, cudaMemcpyAsync(h, tot, sizeof(int), cudaMemcpyDeviceToHost, st));
+	CT_CUDA(c, cudaStreamSynchronize(st));
+	b->rung_begin = beg + h[0];
+	b->tree_valid = false;
+	return CT_OK;
+}
+
+ct_status direct_ewald_run(Ctx* c, Box* b, int64_t nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, double h, double* gx,
+		double* gy, double* gz, double* pot) {
+	cudaStream_t st = c->stream;
+	static ct_p7::EwaldTab tab;
+	ct_p7::ewald_build_indices(tab);
+	ct_status s = CT_OK;
+	float* dreal = (float*) scratch(c, 30, sizeof(tab.real) + sizeof(tab.four), &s);
+	uint32_t* dsk = (uint32_t*) scratch(c, 31, sizeof(uint32_t) * 3 * nsink, &s);
+	double* dout = (double*) scratch(c, 32, sizeof(double) * 4 * nsink + 2 * CT_EWALD_NFOUR * sizeof(double), &s);
+	CT_TRY(s);
+	float* dfour = dreal + 3 * CT_EWALD_NREAL;
+	double* CS = dout + 4 * nsink;
+	CT_CUDA(c, cudaMemcpyAsync(dreal, tab.real, sizeof(tab.real), cudaMemcpyHostToDevice, st));
+	CT_CUDA(c, cudaMemcpyAsync(dfour, tab.four, sizeof(tab.four), cudaMemcpyHostToDevice, st));
+	CT_CUDA(c, cudaMemcpyAsync(dsk, sx, sizeof(uint32_t) * nsink, cudaMemcpyHostToDevice, st));
+	CT_CUDA(c, cudaMemcpyAsync(dsk + nsink, sy, sizeof(uint32_t) * nsink, cudaMemcpyHostToDevice, st));
+	CT_CUDA(c, cudaMemcpyAsync(dsk + 2 * nsink, sz, sizeof(uint32_t) * nsink, cudaMemcpyHostToDevice, st));
+	CT_CUDA(c, cudaMemsetAsync(CS, 0, 2 * CT_EWALD_NFOUR * sizeof(double), st));
+	const int64_t n = b->n;
+	dim3 gsf((unsigned) std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 64)), CT_EWALD_NFOUR);
+	k_struct_factor<<<gsf, 256, 0, st>>>(n, b->x[0], b->x[1], b->x[2], dfour, CS);
+	for (int64_t s0 = 0; s0 < nsink; s0 += 65535) {
+		const int ns = (int) std::min<int64_t>(65535, nsink - s0);
+		k_direct_ewald<<<ns, 256, 0, st>>>(n, b->x[0], b->x[1], b->x[2], dsk + s0, dsk + nsink + s0, dsk + 2 * nsink + s0, h, dreal, dout + 4 * s0);
+	}
+	k_direct_ewald_four<<<(int) ((nsink + 127) / 128), 128, 0, st>>>((int) nsink, dsk, dsk + nsink, dsk + 2 * nsink, dfour, CS, h, dout);
+	CT_CUDA(c, cudaGetLastError());
+	std::vector<double> hout(4 * nsink);
+	CT_CUDA(c, cudaMemcpyAsync(hout.data(), dout, sizeof(double) * 4 * nsink, cudaMemcpyDeviceToHost, st));
+	CT_CUDA(c, cudaStreamSynchronize(st));
+	for (int64_t i = 0; i < nsink; i++) {
+		gx[i] = hout[4 * i];
+		gy[i] = hout[4 * i + 1];
+		gz[i] = hout[4 * i + 2];
+		pot[i] = hout[4 * i + 3];
+	}
+	return CT_OK;
+}
+
+}  // namespace ct
+
+using namespace ct;
+
+extern "C" {
+
+ct_status ct_ctx_create(ct_ctx** out, int device, size_t hbm_budget_bytes, int order) {
+	if (!out || (order != 7 && order != 5)) {
+		return CT_ERR_ARG;
+	}
+	*out = nullptr;
+	Ctx* c = new (std::nothrow) Ctx();
+	if (!c) {
+		return CT_ERR_MEMORY;
+	}
+	c->device = device;
+	c->order = order;
+	c->budget = hbm_budget_bytes;
+	cudaError_t e = cudaSetDevice(device);
+	if (e != cudaSuccess) {
+		delete c;
+		return CT_ERR_CUDA;
+	}
+	cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+	if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+		delete c;
+		return CT_ERR_CUDA;
+	}
+	for (int i = 0; i < 16; i++) {
+		cudaEventCreate(&c->ev[i]);
+	}
+	c->pinned_bytes = 1 << 16;
+	if (cudaMallocHost(&c->pinned, c->pinned_bytes) != cudaSuccess) {
+		delete c;
+		return CT_ERR_MEMORY;
+	}
+	if (dalloc(c, (void**) &c->d_flags, 64 * sizeof(int), "flags") != CT_OK || dalloc(c, (void**) &c->d_counters, 32 * sizeof(double), "counters") != CT_OK) {
+		ct_ctx_destroy((ct_ctx*) c);
+		return CT_ERR_MEMORY;
+	}
+	cudaMemset(c->d_flags, 0, 64 * sizeof(int));
+	const ct_status s = ewald_init(c);
+	if (s != CT_OK) {
+		ct_ctx_destroy((ct_ctx*) c);
+		return s;
+	}
+	*out = (ct_ctx*) c;
+	return CT_OK;
+}
+
+void ct_ctx_destroy(ct_ctx* ctx) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c) {
+		return;
+	}
+	cudaSetDevice(c->device);
+	if (c->stream) {
+		cudaStreamSynchronize(c->stream);
+	}
+	for (size_t i = 0; i < c->boxes.size(); i++) {
+		if (c->boxes[i]) {
+			ct_box_destroy(ctx, (int) i);
+		}
+	}
+	for (auto& s : c->scratch) {
+		dfree(c, s.p, s.bytes);
+	}
+	dfree(c, c->d_flags, 64 * sizeof(int));
+	dfree(c, c->d_counters, 32 * sizeof(double));
+	if (c->pinned) {
+		cudaFreeHost(c->pinned);
+	}
+	for (int i = 0; i < 16; i++) {
+		cudaEventDestroy(c->ev[i]);
+	}
+	if (c->stream) {
+		cudaStreamDestroy(c->stream);
+	}
+	delete c;
+}
+
+const char* ct_last_error(const ct_ctx* ctx) {
+	const Ctx* c = (const Ctx*) ctx;
+	return c ? c->err.c_str() : "no context";
+}
+
+int ct_order(const ct_ctx* ctx) {
+	return ctx ? ((const Ctx*) ctx)->order : 0;
+}
+
+ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c || n < 0 || !box_id || n > (int64_t) INT32_MAX / 2) {
+		return fail(c, CT_ERR_ARG, "ct_box_create: bad arguments");
+	}
+	cudaSetDevice(c->device);
+	Box* b = new (std::nothrow) Box();
+	if (!b) {
+		return fail(c, CT_ERR_MEMORY, "host allocation");
+	}
+	b->n = n;
+	memset(&b->counters, 0, sizeof(b->counters));
+	ct_status s = CT_OK;
+	for (int d = 0; d < 3 && s == CT_OK; d++) {
+		s = dalloc(c, (void**) &b->x[d], sizeof(uint32_t) * n, "positions");
+		if (s == CT_OK) {
+			s = dalloc(c, (void**) &b->v[d], sizeof(float) * n, "velocities");
+		}
+	}
+	if (s == CT_OK) {
+		s = dalloc(c, (void**) &b->rung, n + 16, "rungs");
+	}
+	if (s != CT_OK) {
+		for (int d = 0; d < 3; d++) {
+			dfree(c, b->x[d], sizeof(uint32_t) * n);
+			dfree(c, b->v[d], sizeof(float) * n);
+		}
+		delete b;
+		return s;
+	}
+	int id = -1;
+	for (size_t i = 0; i < c->boxes.size(); i++) {
+		if (!c->boxes[i]) {
+			id = (int) i;
+			break;
+		}
+	}
+	if (id < 0) {
+		id = (int) c->boxes.size();
+		c->boxes.push_back(nullptr);
+	}
+	c->boxes[id] = b;
+	*box_id = id;
+	return CT_OK;
+}
+
+ct_status ct_box_destroy(ct_ctx* ctx, int box_id) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b) {
+		return fail(c, CT_ERR_ARG, "ct_box_destroy: no such box");
+	}
+	cudaStreamSynchronize(c->stream);
+	const int64_t n = b->n;
+	for (int d = 0; d < 3; d++) {
+		dfree(c, b->x[d], sizeof(uint32_t) * n);
+		dfree(c, b->v[d], sizeof(float) * n);
+		dfree(c, b->g[d], sizeof(float) * n);
+	}
+	dfree(c, b->pot, sizeof(float) * n);
+	dfree(c, b->rung, n + 16);
+	const int64_t cap = b->node_cap;
+	dfree(c, b->nodes, sizeof(NodeW) * cap);
+	dfree(c, b->nbox, sizeof(int32_t) * 6 * cap);
+	dfree(c, b->multi, sizeof(float) * NMULT_STRIDE * cap);
+	dfree(c, b->key, sizeof(uint64_t) * cap);
+	dfree(c, b->depth, sizeof(int32_t) * cap);
+	dfree(c, b->parent, sizeof(int32_t) * cap);
+	dfree(c, b->gbox, sizeof(double) * 6 * cap);
+	dfree(c, b->tbox, sizeof(double) * 6 * cap);
+	delete b;
+	c->boxes[box_id] = nullptr;
+	return CT_OK;
+}
+
+int64_t ct_box_size(const ct_ctx* ctx, int box_id) {
+	Box* b = get_box((Ctx*) ctx, box_id);
+	return b ? b->n : -1;
+}
+
+static ct_status upload_impl(Ctx* c, Box* b, const uint32_t* x, const uint32_t* y, const uint32_t* z, const float* vxyz, const int8_t* rung,
+		cudaMemcpyKind kind) {
+	cudaStream_t st = c->stream;
+	const int64_t n = b->n;
+	const uint32_t* src[3] = { x, y, z };
+	for (int d = 0; d < 3; d++) {
+		if (src[d]) {
+			CT_CUDA(c, cudaMemcpyAsync(b->x[d], src[d], sizeof(uint32_t) * n, kind, st));
+		}
+	}
+	if (vxyz && n > 0) {
+		ct_status s = CT_OK;
+		float* tmp = (float*) scratch(c, 33, sizeof(float) * 3 * n, &s);
+		CT_TRY(s);
+		CT_CUDA(c, cudaMemcpyAsync(tmp, vxyz, sizeof(float) * 3 * n, kind, st));
+		k_aos_to_soa<<<grid(c, n, 256), 256, 0, st>>>(n, tmp, b->v[0], b->v[1], b->v[2]);
+	}
+	if (rung) {
+		CT_CUDA(c, cudaMemcpyAsync(b->rung, rung, n, kind, st));
+	}
+	CT_CUDA(c, cudaGetLastError());
+	b->tree_valid = false;
+	b->rung_begin = 0;
+	return CT_OK;
+}
+
+static ct_status download_impl(Ctx* c, Box* b, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz,
+		float* pot, cudaMemcpyKind kind) {
+	cudaStream_t st = c->stream;
+	const int64_t n = b->n;
+	uint32_t* dst[3] = { x, y, z };
+	for (int d = 0; d < 3; d++) {
+		if (dst[d]) {
+			CT_CUDA(c, cudaMemcpyAsync(dst[d], b->x[d], sizeof(uint32_t) * n, kind, st));
+		}
+	}
+	if (vxyz && n > 0) {
+		ct_status s = CT_OK;
+		float* tmp = (float*) scratch(c, 33, sizeof(float) * 3 * n, &s);
+		CT_TRY(s);
+		k_soa_to_aos<<<grid(c, n, 256), 256, 0, st>>>(n, b->v[0], b->v[1], b->v[2], tmp);
+		CT_CUDA(c, cudaMemcpyAsync(vxyz, tmp, sizeof(float) * 3 * n, kind, st));
+	}
+	if (rung) {
+		CT_CUDA(c, cudaMemcpyAsync(rung, b->rung, n, kind, st));
+	}
+	float* gd[4] = { gx, gy, gz, pot };
+	float* gs[4] = { b->g[0], b->g[1], b->g[2], b->pot };
+	for (int d = 0; d < 4; d++) {
+		if (gd[d]) {
+			if (!gs[d]) {
+				return fail(c, CT_ERR_STATE, "forces were not saved (kick with save_force first)");
+			}
+			CT_CUDA(c, cudaMemcpyAsync(gd[d], gs[d], sizeof(float) * n, kind, st));
+		}
+	}
+	CT_CUDA(c, cudaStreamSynchronize(st));
+	return CT_OK;
+}
+
+ct_status ct_box_upload(ct_ctx* ctx, int box_id, const uint32_t* x, const uint32_t* y, const uint32_t* z, const float* vxyz, const int8_t* rung) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b) {
+		return fail(c, CT_ERR_ARG, "ct_box_upload: no such box");
+	}
+	cudaSetDevice(c->device);
+	CT_TRY(upload_impl(c, b, x, y, z, vxyz, rung, cudaMemcpyHostToDevice));
+	CT_CUDA(c, cudaStreamSynchronize(c->stream));
+	return CT_OK;
+}
+
+ct_status ct_box_upload_device(ct_ctx* ctx, int box_id, const uint32_t* x, const uint32_t* y, const uint32_t* z, const float* vxyz, const int8_t* rung) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b) {
+		return fail(c, CT_ERR_ARG, "ct_box_upload_device: no such box");
+	}
+	cudaSetDevice(c->device);
+	return upload_impl(c, b, x, y, z, vxyz, rung, cudaMemcpyDeviceToDevice);
+}
+
+ct_status ct_box_download(ct_ctx* ctx, int box_id, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz,
+		float* pot) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b) {
+		return fail(c, CT_ERR_ARG, "ct_box_download: no such box");
+	}
+	cudaSetDevice(c->device);
+	return download_impl(c, b, x, y, z, vxyz, rung, gx, gy, gz, pot, cudaMemcpyDeviceToHost);
+}
+
+ct_status ct_box_download_device(ct_ctx* ctx, int box_id, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy,
+		float* gz, float* pot) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b) {
+		return fail(c, CT_ERR_ARG, "ct_box_download_device: no such box");
+	}
+	cudaSetDevice(c->device);
+	return download_impl(c, b, x, y, z, vxyz, rung, gx, gy, gz, pot, cudaMemcpyDeviceToDevice);
+}
+
+ct_status ct_sort_by_rung(ct_ctx* ctx, int box_id, int min_rung, int64_t* rung_begin) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || min_rung < 0 || min_rung > 15) {
+		return fail(c, CT_ERR_ARG, "ct_sort_by_rung: bad arguments");
+	}
+	cudaSetDevice(c->device);
+	CT_TRY(sort_by_rung_run(c, b, min_rung));
+	if (rung_begin) {
+		*rung_begin = b->rung_begin;
+	}
+	return CT_OK;
+}
+
+ct_status ct_tree_create(ct_ctx* ctx, int box_id, const ct_tree_params* params, int64_t* node_count) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !params || params->bucket < 1 || !(params->theta > 0.0) || params->hsoft < 0.0) {
+		return fail(c, CT_ERR_ARG, "ct_tree_create: bad arguments");
+	}
+	cudaSetDevice(c->device);
+	cudaEventRecord(c->ev[8], c->stream);
+	CT_TRY(tree_build(c, b, params));
+	cudaEventRecord(c->ev[9], c->stream);
+	cudaEventSynchronize(c->ev[9]);
+	float ms = 0.f;
+	cudaEventElapsedTime(&ms, c->ev[8], c->ev[9]);
+	b->counters.ms_tree = ms;
+	if (node_count) {
+		*node_count = b->nnodes;
+	}
+	return CT_OK;
+}
+
+ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* result) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !params || !(params->theta > 0.f) || !(params->h > 0.f) || params->min_rung < 0 || params->min_rung > 15) {
+		return fail(c, CT_ERR_ARG, "ct_kick: bad arguments");
+	}
+	if (!b->tree_valid) {
+		return fail(c, CT_ERR_STATE, "ct_kick: no valid tree (call ct_tree_create after every upload/drift/sort)");
+	}
+	if (std::fabs((double) params->theta - b->tparams.theta) > 1e-6 * b->tparams.theta) {
+		return fail(c, CT_ERR_ARG, "ct_kick: theta differs from the one the tree was built with");
+	}
+	cudaSetDevice(c->device);
+	if (params->save_force && !b->pot) {
+		for (int d = 0; d < 3; d++) {
+			CT_TRY(dalloc(c, (void**) &b->g[d], sizeof(float) * b->n, "forces"));
+		}
+		CT_TRY(dalloc(c, (void**) &b->pot, sizeof(float) * b->n, "potentials"));
+	}
+	return kick_run(c, b, params, result);
+}
+
+ct_status ct_drift(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !(a > 0.f) || rung < 0 || rung > 127) {
+		return fail(c, CT_ERR_ARG, "ct_drift: bad arguments");
+	}
+	cudaSetDevice(c->device);
+	CT_TRY(drift_run(c, b, rung, a, dt, drag));
+	return CT_OK;
+}
+
+ct_status ct_tree_download(ct_ctx* ctx, int box_id, ct_node* nodes, int64_t max_nodes, int64_t* count) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !count) {
+		return fail(c, CT_ERR_ARG, "ct_tree_download: bad arguments");
+	}
+	if (!b->tree_valid) {
+		return fail(c, CT_ERR_STATE, "ct_tree_download: no valid tree");
+	}
+	*count = b->nnodes;
+	if (!nodes) {
+		return CT_OK;
+	}
+	if (max_nodes < b->nnodes) {
+		return fail(c, CT_ERR_ARG, "ct_tree_download: output too small");
+	}
+	cudaSetDevice(c->device);
+	const int64_t nn = b->nnodes;
+	std::vector<NodeW> w(nn);
+	std::vector<int32_t> bx(6 * nn), dep(nn);
+	std::vector<float> mu(NMULT_STRIDE * nn);
+	std::vector<uint64_t> key(nn);
+	cudaStream_t st = c->stream;
+	CT_CUDA(c, cudaMemcpyAsync(w.data(), b->nodes, sizeof(NodeW) * nn, cudaMemcpyDeviceToHost, st));
+	CT_CUDA(c, cudaMemcpyAsync(bx.data(), b->nbox, sizeof(int32_t) * 6 * nn, cudaMemcpyDeviceToHost, st));
+	CT_CUDA(c, cudaMemcpyAsync(dep.data(), b->depth, sizeof(int32_t) * nn, cudaMemcpyDeviceToHost, st));
+	CT_CUDA(c, cudaMemcpyAsync(mu.data(), b->multi, sizeof(float) * NMULT_STRIDE * nn, cudaMemcpyDeviceToHost, st));
+	CT_CUDA(c, cudaMemcpyAsync(key.data(), b->key, sizeof(uint64_t) * nn, cudaMemcpyDeviceToHost, st));
+	CT_CUDA(c, cudaStreamSynchronize(st));
+	const int nm = c->order == 5 ? 17 : 37;
+	for (int64_t i = 0; i < nn; i++) {
+		ct_node& o = nodes[i];
+		memset(&o, 0, sizeof(o));
+		o.key = key[i];
+		o.part_begin = w[i].pbeg;
+		o.part_end = w[i].pend;
+		o.child_left = w[i].child;
+		o.child_right = w[i].child >= 0 ? w[i].child + 1 : -1;
+		o.pos[0] = w[i].x;
+		o.pos[1] = w[i].y;
+		o.pos[2] = w[i].z;
+		o.radius = w[i].radius;
+		for (int d = 0; d < 3; d++) {
+			o.box_begin[d] = bx[6 * i + d];
+			o.box_end[d] = bx[6 * i + 3 + d];
+		}
+		o.leaf = w[i].flags & 1;
+		o.depth = dep[i];
+		for (int k = 0; k < nm; k++) {
+			o.multi[k] = mu[NMULT_STRIDE * i + k];
+		}
+	}
+	return CT_OK;
+}
+
+ct_status ct_get_counters(ct_ctx* ctx, int box_id, ct_counters* out) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !out) {
+		return fail(c, CT_ERR_ARG, "ct_get_counters: bad arguments");
+	}
+	float ms = 0.f;
+	if (cudaEventQuery(c->ev[7]) == cudaSuccess && cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]) == cudaSuccess) {
+		b->counters.ms_drift = ms;
+	}
+	*out = b->counters;
+	return CT_OK;
+}
+
+ct_status ct_synchronize(ct_ctx* ctx) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c) {
+		return CT_ERR_ARG;
+	}
+	CT_CUDA(c, cudaStreamSynchronize(c->stream));
+	return CT_OK;
+}
+
+ct_status ct_direct_ewald(ct_ctx* ctx, int box_id, int64_t nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, double h, double* gx,
+		double* gy, double* gz, double* pot) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || nsink <= 0 || !sx || !sy || !sz || !gx || !gy || !gz || !pot || !(h > 0.0)) {
+		return fail(c, CT_ERR_ARG, "ct_direct_ewald: bad arguments");
+	}
+	cudaSetDevice(c->device);
+	return direct_ewald_run(c, b, nsink, sx, sy, sz, h, gx, gy, gz, pot);
+}
+
+}  // extern "C"

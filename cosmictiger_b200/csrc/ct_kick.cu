@@ -1,0 +1,1099 @@
+// The kick: dual tree walk, interactions and the leaf kick on the device.
+//
+// Reference: cuda_kick_kernel (src/kick.cu:179-506) walks each work item's subtree depth-first
+// in one warp and evaluates interactions as it goes; the host walks the top of the tree
+// (src/kick.cpp:150-507).  Here the walk is breadth-first over the whole tree, one warp per
+// node, with the reference's opening criteria and list semantics:
+//   Ewald list  (kick.cu:269-329): CC if max(R^2, (0.5-(rs+ro))^2) > ((rs+ro)/theta)^2,
+//                otherwise the children are checked one level down;
+//   direct list (kick.cu:330-431): CC if R > max((rs+ro)/theta, rs+ro+h); for leaf-leaf pairs
+//                P2L (CP) / M2P (PC) by the dpc/dcp and box tests with MIN_PARTS_PCCP;
+//                remaining leaves are P2P, other nodes are opened; a leaf re-checks the
+//                children it opens until none remain; a non-leaf passes children and leaves
+//                down to both of its children.
+// Every node's lists land contiguously in global memory (per-warp staging), so that the
+// interaction kernels that follow read them with one pass per node:
+//   k_m2l        Ewald and direct M2L plus P2L into the node's own expansion delta (warp per
+//                node, lanes over sources, butterfly reduction; gravity.cu:44-155,213-244);
+//   k_l2l        top-down L2L: L(node) = L2L(L(parent)) + delta (kick.cu:246-258);
+//   k_leaf       M2P, P2P (sources staged in shared memory as floats relative to the leaf
+//                centre, compensated per-batch accumulation), L2P and the kick
+//                (gravity.cu:157-211,246-404, kick.cu:53-177).
+#include <cub/cub.cuh>
+
+#include "ct_internal.cuh"
+#include "ct_ops.cuh"
+
+namespace ct {
+
+__constant__ ct_p7::EwaldTab c_tab7;
+__constant__ ct_p5::EwaldTab c_tab5;
+
+template<class Ops> __device__ __forceinline__ const typename Ops::Tab& ewald_tab();
+template<> __device__ __forceinline__ const ct_p7::EwaldTab& ewald_tab<Ops7>() {
+	return c_tab7;
+}
+template<> __device__ __forceinline__ const ct_p5::EwaldTab& ewald_tab<Ops5>() {
+	return c_tab5;
+}
+
+namespace {
+
+// ---------------------------------------------------------------- Ewald tables (FP64 on the device)
+__global__ void k_ewald_four7(ct_p7::EwaldTab* t) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < CT_EWALD_NFOUR) {
+		double E[ct_p7::NEXP];
+		ct_p7::ewald_four_entry(E, t->four[i][0], t->four[i][1], t->four[i][2]);
+		for (int k = 0; k < ct_p7::NEXP; k++) {
+			t->four_exp[i][k] = (float) E[k];
+		}
+	}
+	if (i < ct_p7::NFULL) {
+		t->D0[i] = (float) ct_p7::ewald_d0_entry(i);
+	}
+}
+__global__ void k_ewald_four5(ct_p5::EwaldTab* t) {
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < CT_EWALD_NFOUR) {
+		double E[ct_p5::NEXP];
+		ct_p5::ewald_four_entry(E, t->four[i][0], t->four[i][1], t->four[i][2]);
+		for (int k = 0; k < ct_p5::NEXP; k++) {
+			t->four_exp[i][k] = (float) E[k];
+		}
+	}
+	if (i < ct_p5::NFULL) {
+		t->D0[i] = (float) ct_p5::ewald_d0_entry(i);
+	}
+}
+
+// ---------------------------------------------------------------- walk
+constexpr int WALK_TPB = 128;
+constexpr int NLIST = 8;  // per-warp staging arrays
+enum {
+	S_ECC = 0, S_EOUT, S_DCC, S_CP, S_PC, S_LEAF, S_NEXT0, S_NEXT1
+};
+
+struct WalkOut {
+	// per node, indexed by node id: {offset, count} pairs
+	int2* ecc;   // Ewald CC sources
+	int2* dcc;   // direct CC sources
+	int2* cp;    // leaves: P2L source leaves
+	int2* pc;    // leaves: M2P source nodes
+	int2* pp;    // leaves: P2P source leaves
+	int2* eout;  // non-leaves: Ewald checks passed to the children
+	int2* dout;  // non-leaves: direct checks passed to the children
+	int* ecc_list;
+	int* dcc_list;
+	int* cp_list;
+	int* pc_list;
+	int* pp_list;
+	int* pass_cur;   // pass-down lists of this level (eout/dout)
+	int* pass_prev;  // pass-down lists of the level above
+	unsigned long long* cursor;  // [0] ecc [1] dcc [2] cp [3] pc [4] pp [5] pass (this level)
+	long long cap_cc, cap_leaf, cap_pass;
+	int* stage;   // per-warp staging, NLIST * stage_cap ints per warp
+	int stage_cap;
+	int* flags;   // [0] overflow [1] dropped Ewald check
+};
+
+struct WalkParams {
+	float thetainv;
+	float h;
+	int level0;
+};
+
+__device__ __forceinline__ float sqrf3(float a, float b, float c) {
+	return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
+
+// distance(fixed32 b, range_fixed a) of range.hpp:447-458, negated argument order
+__device__ __forceinline__ float dist_rf(uint32_t b, int32_t a) {
+	float f = __dsub_rn(__dmul_rn((double) a, 1.0 / 536870912.0), fixed_to_double(b));
+	f = (float) __dsub_rn((double) f, (double) (f > 0.5f));
+	f = (float) __dadd_rn((double) f, (double) (f < -0.5f));
+	return -f;
+}
+
+// box_intersects_sphere (range.hpp:459-466)
+__device__ __forceinline__ bool box_sphere(const int32_t* bx, uint32_t x, uint32_t y, uint32_t z, float r) {
+	const uint32_t X[3] = { x, y, z };
+	float d2 = 0.0f;
+	for (int d = 0; d < 3; d++) {
+		const float a = dist_rf(X[d], bx[d]);
+		const float b = dist_rf(X[d], bx[3 + d]);
+		const float d2b = __fmul_rn(a, a), d2e = __fmul_rn(b, b);
+		const int32_t xr = (int32_t) (X[d] >> 3);
+		const int outside = (xr < bx[d]) + (xr > bx[3 + d]);
+		d2 = __fadd_rn(d2, __fmul_rn((float) outside, fminf(d2b, d2e)));
+	}
+	return d2 < __fmul_rn(r, r);
+}
+
+// Warp-compacted append of `n` (0..2) values per lane to a staging array.
+__device__ __forceinline__ void stage_push(int* arr, int& cnt, int cap, int lane, int n, int v0, int v1, int* ovf) {
+	const unsigned m1 = __ballot_sync(0xffffffffu, n >= 1);
+	const unsigned m2 = __ballot_sync(0xffffffffu, n >= 2);
+	const unsigned lt = (1u << lane) - 1u;
+	const int off = __popc(m1 & lt) + __popc(m2 & lt);
+	const int tot = __popc(m1) + __popc(m2);
+	if (n >= 1) {
+		const int p = cnt + off;
+		if (p < cap) {
+			arr[p] = v0;
+		} else {
+			*ovf = 1;
+		}
+		if (n >= 2) {
+			if (p + 1 < cap) {
+				arr[p + 1] = v1;
+			} else {
+				*ovf = 1;
+			}
+		}
+	}
+	cnt += tot;
+}
+
+// Copy a staged list to global memory; returns {offset, count}.
+__device__ __forceinline__ int2 flush(const int* src, int cnt, int cap, int* dst, unsigned long long* cursor, long long dcap, int lane, int* ovf) {
+	cnt = min(cnt, cap);
+	unsigned long long off = 0;
+	if (lane == 0 && cnt) {
+		off = atomicAdd(cursor, (unsigned long long) cnt);
+	}
+	off = __shfl_sync(0xffffffffu, off, 0);
+	if ((long long) (off + cnt) > dcap) {
+		if (lane == 0) {
+			atomicOr(ovf, 1);
+		}
+		return make_int2(0, 0);
+	}
+	for (int i = lane; i < cnt; i += 32) {
+		dst[off + i] = src[i];
+	}
+	return make_int2((int) off, cnt);
+}
+
+__global__ void __launch_bounds__(WALK_TPB) k_walk(int64_t lb, int64_t le, const NodeW* __restrict__ nodes, const int32_t* __restrict__ nbox,
+		const int32_t* __restrict__ parent, WalkOut o, WalkParams p) {
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nw = (gridDim.x * blockDim.x) >> 5;
+	int* st = o.stage + (size_t) gw * NLIST * o.stage_cap;
+	const int cap = o.stage_cap;
+	int* sl[NLIST];
+	for (int k = 0; k < NLIST; k++) {
+		sl[k] = st + k * cap;
+	}
+	int ovf = 0, dropped = 0;
+	const float thetainv = p.thetainv, h = p.h;
+	for (int64_t si = lb + gw; si < le; si += nw) {
+		const NodeW self = nodes[si];
+		const int nsinks = self.pend - self.pbeg;
+		const bool sleaf = self.flags & 1;
+		int2 z2 = make_int2(0, 0);
+		if (nsinks == 0) {
+			if (lane == 0) {
+				o.ecc[si] = z2;
+				o.dcc[si] = z2;
+				if (sleaf) {
+					o.cp[si] = z2;
+					o.pc[si] = z2;
+					o.pp[si] = z2;
+				} else {
+					o.eout[si] = z2;
+					o.dout[si] = z2;
+				}
+			}
+			continue;
+		}
+		// input check lists: the parent's pass-down lists, or {root} at the root
+		const int* ein;
+		const int* din;
+		int ne, nd;
+		int root_list = 0;
+		if (si == 0) {
+			ein = din = &root_list;
+			ne = nd = 1;
+		} else {
+			const int pa = parent[si];
+			const int2 e = o.eout[pa], d = o.dout[pa];
+			ein = o.pass_prev + e.x;
+			ne = e.y;
+			din = o.pass_prev + d.x;
+			nd = d.y;
+		}
+		int32_t sbox[6];
+		if (sleaf) {
+			for (int d = 0; d < 6; d++) {
+				sbox[d] = nbox[6 * si + d];
+			}
+		}
+		const float rs = self.radius;
+		// ---- Ewald list: one pass
+		int n_ecc = 0, n_eout = 0;
+		for (int j0 = 0; j0 < ne; j0 += 32) {
+			const int j = j0 + lane;
+			int cc = 0, nx = 0, c = 0, c0 = 0;
+			if (j < ne) {
+				c = ein[j];
+				const NodeW ot = nodes[c];
+				if (ot.pend > ot.pbeg) {
+					const float dx = fixed_dist(self.x, ot.x), dy = fixed_dist(self.y, ot.y), dz = fixed_dist(self.z, ot.z);
+					float R2 = sqrf3(dx, dy, dz);
+					const float t = fmaxf(__fsub_rn(0.5f, __fadd_rn(rs, ot.radius)), 0.f);
+					R2 = fmaxf(R2, __fmul_rn(t, t));
+					const float dcc = __fmul_rn(__fadd_rn(rs, ot.radius), thetainv);
+					cc = R2 > __fmul_rn(dcc, dcc);
+					if (!cc) {
+						if (ot.child >= 0 && !sleaf) {
+							nx = 2;
+							c0 = ot.child;
+						} else {
+							dropped = 1;
+						}
+					}
+				}
+			}
+			stage_push(sl[S_ECC], n_ecc, cap, lane, cc, c, 0, &ovf);
+			stage_push(sl[S_EOUT], n_eout, cap, lane, nx, c0, c0 + 1, &ovf);
+		}
+		// ---- direct list (leaf: iterate over the children it opens)
+		int n_dcc = 0, n_cp = 0, n_pc = 0, n_leaf = 0, n_next = 0;
+		const int* cur = din;
+		int ncur = nd;
+		int which = 0;
+		while (true) {
+			int* nxt = sl[S_NEXT0 + which];
+			n_next = 0;
+			for (int j0 = 0; j0 < ncur; j0 += 32) {
+				const int j = j0 + lane;
+				int kind = -1, c = 0;  // 0 cc 1 cp 2 pc 3 leaf 4 next
+				int c0 = 0;
+				if (j < ncur) {
+					c = cur[j];
+					const NodeW ot = nodes[c];
+					const int onp = ot.pend - ot.pbeg;
+					if (onp) {
+						const float dx = fixed_dist(self.x, ot.x), dy = fixed_dist(self.y, ot.y), dz = fixed_dist(self.z, ot.z);
+						const float R2 = sqrf3(dx, dy, dz);
+						const float rsum = __fadd_rn(rs, ot.radius);
+						const float mind = __fadd_rn(rsum, h);
+						const float dcc = fmaxf(__fmul_rn(rsum, thetainv), mind);
+						const bool oleaf = ot.flags & 1;
+						bool sw_cc = R2 > __fmul_rn(dcc, dcc), sw_cp = false, sw_pc = false;
+						if (!sw_cc && oleaf && sleaf) {
+							const float dcp = fmaxf(__fadd_rn(__fmul_rn(rs, thetainv), ot.radius), mind);
+							const float dpc = fmaxf(__fadd_rn(rs, __fmul_rn(ot.radius, thetainv)), mind);
+							sw_pc = (R2 > __fmul_rn(dpc, dpc) || !box_sphere(sbox, ot.x, ot.y, ot.z, fmaxf(__fmul_rn(thetainv, ot.radius), h)))
+									&& nsinks >= MIN_PARTS_PCCP;
+							int32_t obox[6];
+							for (int d = 0; d < 6; d++) {
+								obox[d] = nbox[6 * (int64_t) c + d];
+							}
+							sw_cp = (R2 > __fmul_rn(dcp, dcp) || !box_sphere(obox, self.x, self.y, self.z, fmaxf(__fmul_rn(thetainv, rs), h)))
+									&& onp >= MIN_PARTS_PCCP;
+							if (sw_pc && sw_cp) {
+								if (nsinks < onp) {
+									sw_cp = false;
+								} else if (nsinks > onp) {
+									sw_pc = false;
+								} else {
+									sw_cp = sw_pc = false;
+								}
+							}
+						}
+						if (sw_cc) {
+							kind = 0;
+						} else if (sw_cp) {
+							kind = 1;
+						} else if (sw_pc) {
+							kind = 2;
+						} else if (oleaf) {
+							kind = 3;
+						} else {
+							kind = 4;
+							c0 = ot.child;
+						}
+					}
+				}
+				stage_push(sl[S_DCC], n_dcc, cap, lane, kind == 0, c, 0, &ovf);
+				stage_push(sl[S_CP], n_cp, cap, lane, kind == 1, c, 0, &ovf);
+				stage_push(sl[S_PC], n_pc, cap, lane, kind == 2, c, 0, &ovf);
+				stage_push(sl[S_LEAF], n_leaf, cap, lane, kind == 3, c, 0, &ovf);
+				stage_push(nxt, n_next, cap, lane, kind == 4 ? 2 : 0, c0, c0 + 1, &ovf);
+			}
+			__syncwarp();
+			if (sleaf && n_next > 0) {
+				cur = nxt;
+				ncur = min(n_next, cap);
+				which ^= 1;
+				continue;
+			}
+			break;
+		}
+		__syncwarp();
+		// ---- flush to global lists
+		const int2 ecc = flush(sl[S_ECC], n_ecc, cap, o.ecc_list, o.cursor + 0, o.cap_cc, lane, o.flags);
+		const int2 dcc = flush(sl[S_DCC], n_dcc, cap, o.dcc_list, o.cursor + 1, o.cap_cc, lane, o.flags);
+		if (lane == 0) {
+			o.ecc[si] = ecc;
+			o.dcc[si] = dcc;
+		}
+		if (sleaf) {
+			const int2 cp = flush(sl[S_CP], n_cp, cap, o.cp_list, o.cursor + 2, o.cap_leaf, lane, o.flags);
+			const int2 pc = flush(sl[S_PC], n_pc, cap, o.pc_list, o.cursor + 3, o.cap_leaf, lane, o.flags);
+			const int2 pp = flush(sl[S_LEAF], n_leaf, cap, o.pp_list, o.cursor + 4, o.cap_leaf, lane, o.flags);
+			if (lane == 0) {
+				o.cp[si] = cp;
+				o.pc[si] = pc;
+				o.pp[si] = pp;
+			}
+		} else {
+			// Ewald pass-down: children of the opened checks
+			const int2 eo = flush(sl[S_EOUT], n_eout, cap, o.pass_cur, o.cursor + 5, o.cap_pass, lane, o.flags);
+			// direct pass-down: children of opened checks, then the leaf checks (kick.cu:424-430)
+			const int nn = min(n_next, cap), nl = min(n_leaf, cap);
+			unsigned long long off = 0;
+			if (lane == 0 && nn + nl) {
+				off = atomicAdd(o.cursor + 5, (unsigned long long) (nn + nl));
+			}
+			off = __shfl_sync(0xffffffffu, off, 0);
+			int2 dout = make_int2(0, 0);
+			if ((long long) (off + nn + nl) > o.cap_pass) {
+				if (lane == 0) {
+					atomicOr(o.flags, 1);
+				}
+			} else {
+				const int* nxt = sl[S_NEXT0 + which];
+				for (int i = lane; i < nn; i += 32) {
+					o.pass_cur[off + i] = nxt[i];
+				}
+				for (int i = lane; i < nl; i += 32) {
+					o.pass_cur[off + nn + i] = sl[S_LEAF][i];
+				}
+				dout = make_int2((int) off, nn + nl);
+			}
+			if (lane == 0) {
+				o.eout[si] = eo;
+				o.dout[si] = dout;
+			}
+		}
+		__syncwarp();
+	}
+	if (ovf) {
+		atomicOr(o.flags, 1);
+	}
+	if (dropped) {
+		atomicOr(o.flags + 1, 1);
+	}
+}
+
+// ---------------------------------------------------------------- M2L / P2L
+template<int N>
+__device__ __forceinline__ void warp_reduce_arr(float* L) {
+	for (int o = 16; o; o >>= 1) {
+		for (int i = 0; i < N; i++) {
+			L[i] += __shfl_xor_sync(0xffffffffu, L[i], o);
+		}
+	}
+}
+
+// Ewald M2L for every node: dL = sum over the Ewald CC list.
+template<class Ops>
+__global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi, const int2* __restrict__ ecc,
+		const int* __restrict__ ecc_list, float* __restrict__ dL, int do_phi, double* counters) {
+	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nw = (gridDim.x * blockDim.x) >> 5;
+	double icnt_tot = 0;
+	for (int64_t si = gw; si < nn; si += nw) {
+		const int2 lst = ecc[si];
+		if (lst.y == 0) {
+			if (lane == 0) {
+				for (int i = 0; i < NE; i++) {
+					dL[NEXP_STRIDE * si + i] = 0.f;
+				}
+			}
+			continue;
+		}
+		const NodeW self = nodes[si];
+		float L[NE];
+		for (int i = 0; i < NE; i++) {
+			L[i] = 0.f;
+		}
+		for (int j = lane; j < lst.y; j += 32) {
+			const int c = ecc_list[lst.x + j];
+			const NodeW ot = nodes[c];
+			float M[NM], D[NE];
+			const float4* mp = (const float4*) (multi + (size_t) NMULT_STRIDE * c);
+#pragma unroll
+			for (int k = 0; k < (NM + 3) / 4; k++) {
+				const float4 v = __ldg(mp + k);
+				if (4 * k + 0 < NM) M[4 * k + 0] = v.x;
+				if (4 * k + 1 < NM) M[4 * k + 1] = v.y;
+				if (4 * k + 2 < NM) M[4 * k + 2] = v.z;
+				if (4 * k + 3 < NM) M[4 * k + 3] = v.w;
+			}
+			const int ic = Ops::ewald(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z), ewald_tab<Ops>());
+			icnt_tot += ic;
+			Ops::m2l(L, M, D, do_phi != 0);
+		}
+		warp_reduce_arr<NE>(L);
+		if (lane == 0) {
+			for (int i = 0; i < NE; i++) {
+				dL[NEXP_STRIDE * si + i] = L[i];
+			}
+		}
+	}
+	icnt_tot += __shfl_xor_sync(0xffffffffu, icnt_tot, 16);
+	icnt_tot += __shfl_xor_sync(0xffffffffu, icnt_tot, 8);
+	icnt_tot += __shfl_xor_sync(0xffffffffu, icnt_tot, 4);
+	icnt_tot += __shfl_xor_sync(0xffffffffu, icnt_tot, 2);
+	icnt_tot += __shfl_xor_sync(0xffffffffu, icnt_tot, 1);
+	if (lane == 0 && icnt_tot > 0) {
+		atomicAdd(counters + 0, icnt_tot);
+	}
+}
+
+// Direct M2L and P2L: dL += sum over the direct CC list and the CP source particles.
+template<class Ops>
+__global__ void __launch_bounds__(128) k_m2l_direct(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi,
+		const int2* __restrict__ dcc, const int* __restrict__ dcc_list, const int2* __restrict__ cp, const int* __restrict__ cp_list,
+		const uint32_t* __restrict__ x0, const uint32_t* __restrict__ x1, const uint32_t* __restrict__ x2, float* __restrict__ dL, int do_phi,
+		double* counters) {
+	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nw = (gridDim.x * blockDim.x) >> 5;
+	double ncp = 0;
+	for (int64_t si = gw; si < nn; si += nw) {
+		const int2 lst = dcc[si];
+		const NodeW self = nodes[si];
+		const bool leaf = self.flags & 1;
+		const int2 cpl = leaf ? cp[si] : make_int2(0, 0);
+		if (lst.y == 0 && cpl.y == 0) {
+			continue;
+		}
+		float L[NE];
+		for (int i = 0; i < NE; i++) {
+			L[i] = 0.f;
+		}
+		for (int j = lane; j < lst.y; j += 32) {
+			const int c = dcc_list[lst.x + j];
+			const NodeW ot = nodes[c];
+			float M[NM], D[NE];
+			const float4* mp = (const float4*) (multi + (size_t) NMULT_STRIDE * c);
+#pragma unroll
+			for (int k = 0; k < (NM + 3) / 4; k++) {
+				const float4 v = __ldg(mp + k);
+				if (4 * k + 0 < NM) M[4 * k + 0] = v.x;
+				if (4 * k + 1 < NM) M[4 * k + 1] = v.y;
+				if (4 * k + 2 < NM) M[4 * k + 2] = v.z;
+				if (4 * k + 3 < NM) M[4 * k + 3] = v.w;
+			}
+			Ops::greens(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z));
+			Ops::m2l(L, M, D, do_phi != 0);
+		}
+		// P2L: each source particle's Green's function added to the expansion (gravity.cu:134-144)
+		for (int q = 0; q < cpl.y; q++) {
+			const NodeW src = nodes[cp_list[cpl.x + q]];
+			for (int k = src.pbeg + lane; k < src.pend; k += 32) {
+				float D[NE];
+				Ops::greens(D, fixed_dist(self.x, x0[k]), fixed_dist(self.y, x1[k]), fixed_dist(self.z, x2[k]));
+				for (int i = 0; i < NE; i++) {
+					L[i] += D[i];
+				}
+			}
+			ncp += src.pend - src.pbeg;
+		}
+		warp_reduce_arr<NE>(L);
+		if (lane == 0) {
+			for (int i = 0; i < NE; i++) {
+				dL[NEXP_STRIDE * si + i] += L[i];
+			}
+		}
+	}
+	if (lane == 0 && ncp > 0) {
+		atomicAdd(counters + 1, ncp);
+	}
+}
+
+// ---------------------------------------------------------------- L2L (top-down, one level)
+template<class Ops>
+__global__ void k_l2l(int64_t lb, int64_t le, const NodeW* __restrict__ nodes, const int32_t* __restrict__ parent, const float* __restrict__ dL,
+		float* __restrict__ Lx, int do_phi) {
+	constexpr int NE = Ops::NEXP;
+	for (int64_t i = lb + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < le; i += (int64_t) gridDim.x * blockDim.x) {
+		float out[NE];
+		const float* d = dL + NEXP_STRIDE * i;
+		if (i == 0) {
+			for (int k = 0; k < NE; k++) {
+				out[k] = d[k];
+			}
+		} else {
+			const int pa = parent[i];
+			const NodeW nd = nodes[i], pn = nodes[pa];
+			float La[NE];
+			const float* src = Lx + NEXP_STRIDE * (int64_t) pa;
+			for (int k = 0; k < NE; k++) {
+				La[k] = src[k];
+			}
+			Ops::l2l(out, La, fixed_dist(nd.x, pn.x), fixed_dist(nd.y, pn.y), fixed_dist(nd.z, pn.z), do_phi != 0);
+			for (int k = 0; k < NE; k++) {
+				out[k] += d[k];
+			}
+		}
+		float* dst = Lx + NEXP_STRIDE * i;
+		for (int k = 0; k < NE; k++) {
+			dst[k] = out[k];
+		}
+	}
+}
+
+// ---------------------------------------------------------------- leaf kernel
+constexpr int LEAF_TPB = 128;
+constexpr int PP_BATCH = 1024;
+
+struct LeafArgs {
+	const NodeW* nodes;
+	const float* multi;
+	const float* Lx;
+	const int64_t* leaves;
+	int64_t nleaves;
+	const int2* pc;
+	const int* pc_list;
+	const int2* pp;
+	const int* pp_list;
+	const uint32_t* x[3];
+	float* v[3];
+	int8_t* rung;
+	float* g[3];
+	float* pot;
+	ct_kick_params kp;
+	int compensated;
+	double* sums;  // [0] pot [1] kin [2] dkin [3] xmom [4] ymom [5] zmom [6] nmom [7] pp pairs [8] pc pairs
+	int* max_rung;
+};
+
+__device__ __forceinline__ void ksum(float& s, float& comp, float v) {
+	// Neumaier-compensated running sum of per-batch partial forces
+	const float t = s + v;
+	if (fabsf(s) >= fabsf(v)) {
+		comp += (s - t) + v;
+	} else {
+		comp += (v - t) + s;
+	}
+	s = t;
+}
+
+template<class Ops>
+__global__ void __launch_bounds__(LEAF_TPB) k_leaf(LeafArgs a) {
+	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
+	__shared__ float4 src[PP_BATCH];
+	__shared__ float s_mp[NM];
+	__shared__ uint32_t s_mpos[3];
+	__shared__ double s_red[LEAF_TPB / 32][9];
+	const int tid = threadIdx.x;
+	const auto& kp = a.kp;
+	const float h = kp.h;
+	const float h2 = h * h;
+	const float hinv = 1.f / h;
+	const float h2inv = hinv * hinv;
+	const float h3inv = h2inv * hinv;
+	const float self_phi = 693.f / 256.f;
+	double acc[9];
+	for (int k = 0; k < 9; k++) {
+		acc[k] = 0.0;
+	}
+	int maxr = 0;
+	for (int64_t li = blockIdx.x; li < a.nleaves; li += gridDim.x) {
+		const int64_t si = a.leaves[li];
+		const NodeW self = a.nodes[si];
+		const int nsink = self.pend - self.pbeg;
+		const int2 ppl = a.pp[si];
+		const int2 pcl = a.pc[si];
+		for (int s0 = 0; s0 < nsink; s0 += LEAF_TPB) {
+			const int k = s0 + tid;
+			const bool active = k < nsink;
+			const int snk = self.pbeg + k;
+			uint32_t X[3] = { self.x, self.y, self.z };
+			if (active) {
+				X[0] = a.x[0][snk];
+				X[1] = a.x[1][snk];
+				X[2] = a.x[2][snk];
+			}
+			// sink relative to the leaf centre
+			const float kx = fixed_dist(X[0], self.x), ky = fixed_dist(X[1], self.y), kz = fixed_dist(X[2], self.z);
+			float Fx = 0.f, Fy = 0.f, Fz = 0.f, Fp = self_phi * hinv;
+			// ---- M2P (gravity.cu:157-211): source multipoles at this sink
+			for (int q = 0; q < pcl.y; q++) {
+				const int c = a.pc_list[pcl.x + q];
+				__syncthreads();
+				if (tid < NM) {
+					s_mp[tid] = a.multi[(size_t) NMULT_STRIDE * c + tid];
+				}
+				if (tid == 0) {
+					const NodeW ot = a.nodes[c];
+					s_mpos[0] = ot.x;
+					s_mpos[1] = ot.y;
+					s_mpos[2] = ot.z;
+				}
+				__syncthreads();
+				if (active) {
+					float D[NE], M[NM], L2[5] = { 0.f, 0.f, 0.f, 0.f, 0.f };
+					for (int i = 0; i < NM; i++) {
+						M[i] = s_mp[i];
+					}
+					Ops::greens(D, fixed_dist(X[0], s_mpos[0]), fixed_dist(X[1], s_mpos[1]), fixed_dist(X[2], s_mpos[2]));
+					Ops::m2l2(L2, M, D, kp.do_phi != 0);
+					Fx -= 1e6f * L2[1];
+					Fy -= 1e6f * L2[2];
+					Fz -= 1e6f * L2[3];
+					Fp += 1e3f * L2[0];
+				}
+			}
+			if (active) {
+				acc[8] += pcl.y;
+			}
+			// ---- P2P (gravity.cu:246-404)
+			float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+			float cx = 0.f, cy = 0.f, cz = 0.f, cpot = 0.f;
+			int q = 0;          // index in the P2P list
+			int qoff = 0;       // particles of list entry q already staged
+			int64_t npairs = 0;
+			while (q < ppl.y) {
+				__syncthreads();
+				// stage up to PP_BATCH sources (relative to the leaf centre)
+				int nb = 0;
+				while (nb < PP_BATCH && q < ppl.y) {
+					const NodeW ot = a.nodes[a.pp_list[ppl.x + q]];
+					const int avail = (ot.pend - ot.pbeg) - qoff;
+					const int take = min(avail, PP_BATCH - nb);
+					for (int j = tid; j < take; j += LEAF_TPB) {
+						const int pi = ot.pbeg + qoff + j;
+						src[nb + j] = make_float4(fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z), 0.f);
+					}
+					nb += take;
+					qoff += take;
+					if (qoff == ot.pend - ot.pbeg) {
+						q++;
+						qoff = 0;
+					}
+				}
+				__syncthreads();
+				if (active) {
+					float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
+					for (int j = 0; j < nb; j++) {
+						const float4 s = src[j];
+						const float dx = kx - s.x, dy = ky - s.y, dz = kz - s.z;
+						const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+						float r1inv, r3inv;
+						if (r2 > h2) {
+							r1inv = rsqrtf(r2);
+							r3inv = r1inv * r1inv * r1inv;
+						} else {
+							// Ferrer softening kernel (gravity.hpp:73-96)
+							const float q2 = r2 * h2inv;
+							float f = 315.f / 128.f;
+							f = fmaf(f, q2, -385.f / 32.f);
+							f = fmaf(f, q2, 1485.f / 64.f);
+							f = fmaf(f, q2, -693.f / 32.f);
+							f = fmaf(f, q2, 1155.f / 128.f);
+							r3inv = f * h3inv;
+							float ph = -63.f / 256.f;
+							ph = fmaf(ph, q2, 385.f / 256.f);
+							ph = fmaf(ph, q2, -495.f / 128.f);
+							ph = fmaf(ph, q2, 693.f / 128.f);
+							ph = fmaf(ph, q2, -1155.f / 256.f);
+							ph = fmaf(ph, q2, 693.f / 256.f);
+							r1inv = ph * hinv;
+						}
+						fx = fmaf(dx, r3inv, fx);
+						fy = fmaf(dy, r3inv, fy);
+						fz = fmaf(dz, r3inv, fz);
+						pt -= r1inv;
+					}
+					if (a.compensated) {
+						ksum(sx, cx, fx);
+						ksum(sy, cy, fy);
+						ksum(sz, cz, fz);
+						ksum(sp, cpot, pt);
+					} else {
+						sx += fx;
+						sy += fy;
+						sz += fz;
+						sp += pt;
+					}
+					npairs += nb;
+				}
+			}
+			if (active) {
+				Fx -= sx + cx;
+				Fy -= sy + cy;
+				Fz -= sz + cz;
+				Fp += sp + cpot;
+				acc[7] += (double) npairs;
+				// ---- L2P and the kick (kick.cu:53-177)
+				float La[NE], L2[5];
+				const float* Lsrc = a.Lx + (size_t) NEXP_STRIDE * si;
+				for (int i = 0; i < NE; i++) {
+					La[i] = Lsrc[i];
+				}
+				Ops::l2p(L2, La, kx, ky, kz, kp.do_phi != 0);
+				Fp += 1e3f * L2[0];
+				Fx -= 1e6f * L2[1];
+				Fy -= 1e6f * L2[2];
+				Fz -= 1e6f * L2[3];
+				Fz *= kp.GM;
+				Fy *= kp.GM;
+				Fx *= kp.GM;
+				Fp *= kp.GM;
+				float vx = a.v[0][snk], vy = a.v[1][snk], vz = a.v[2][snk];
+				const float kin0 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
+				const float sgn = kp.sign * (kp.top ? 1.f : -1.f);
+				const float rdt = 1.0f / (float) (1 << kp.min_rung);
+				if (kp.ascending) {
+					const float dt = 0.5f * rdt * kp.t0;
+					if (!kp.first_call) {
+						vx = fmaf(sgn * Fx, dt, vx);
+						vy = fmaf(sgn * Fy, dt, vy);
+						vz = fmaf(sgn * Fz, dt, vz);
+					}
+				}
+				acc[1] += 0.5f * (vx * vx + vy * vy + vz * vz);
+				acc[3] += vx;
+				acc[4] += vy;
+				acc[5] += vz;
+				acc[6] += sqrtf(vx * vx + vy * vy + vz * vz);
+				if (kp.save_force) {
+					a.g[0][snk] = Fx;
+					a.g[1][snk] = Fy;
+					a.g[2][snk] = Fz;
+					a.pot[snk] = Fp;
+				}
+				if (kp.descending) {
+					const float g2 = Fx * Fx + Fy * Fy + Fz * Fz;
+					float dt = fminf(kp.eta * sqrtf(kp.a * h * rsqrtf(g2)), kp.t0);
+					dt = fminf(kp.max_dt, dt);
+					int r = a.rung[snk];
+					r = max(kp.min_rung + int((int) ceilf(log2f(kp.t0 / dt)) > kp.min_rung), r - 1);
+					r = max(0, min(r, 15));
+					a.rung[snk] = (int8_t) r;
+					maxr = max(maxr, r);
+					dt = 0.5f * rdt * kp.t0;
+					vx = fmaf(sgn * Fx, dt, vx);
+					vy = fmaf(sgn * Fy, dt, vy);
+					vz = fmaf(sgn * Fz, dt, vz);
+				}
+				const float kin1 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
+				a.v[0][snk] = vx;
+				a.v[1][snk] = vy;
+				a.v[2][snk] = vz;
+				acc[0] += 0.5f * Fp;
+				acc[2] += kin1 - kin0;
+			}
+		}
+	}
+	// block reduction of the sums
+	const int lane = tid & 31, w = tid >> 5;
+	for (int k = 0; k < 9; k++) {
+		double v = acc[k];
+		for (int o = 16; o; o >>= 1) {
+			v += __shfl_xor_sync(0xffffffffu, v, o);
+		}
+		if (lane == 0) {
+			s_red[w][k] = v;
+		}
+	}
+	for (int o = 16; o; o >>= 1) {
+		maxr = max(maxr, __shfl_xor_sync(0xffffffffu, maxr, o));
+	}
+	__syncthreads();
+	if (tid < 9) {
+		double v = 0;
+		for (int q = 0; q < LEAF_TPB / 32; q++) {
+			v += s_red[q][tid];
+		}
+		atomicAdd(a.sums + tid, v);
+	}
+	if (lane == 0 && maxr > 0) {
+		atomicMax(a.max_rung, maxr);
+	}
+}
+
+__global__ void k_collect_leaves(int64_t nn, const NodeW* nodes, int64_t* leaves, unsigned long long* count) {
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nn; i += (int64_t) gridDim.x * blockDim.x) {
+		const NodeW nd = nodes[i];
+		if ((nd.flags & 1) && nd.pend > nd.pbeg) {
+			const unsigned long long p = atomicAdd(count, 1ull);
+			leaves[p] = i;
+		}
+	}
+}
+
+// ---------------------------------------------------------------- host driver
+struct KickBuffers {
+	int2* per_node = nullptr;  // 7 arrays of nnodes
+	size_t per_node_n = 0;
+	int* cc = nullptr;         // ecc + dcc lists
+	size_t cc_n = 0;
+	long long cap_cc = 0;
+	int* leafl = nullptr;      // cp + pc + pp lists
+	size_t leaf_n = 0;
+	long long cap_leaf = 0;
+	int* pass = nullptr;       // two pass-down buffers
+	size_t pass_n = 0;
+	long long cap_pass = 0;
+	int* stage = nullptr;
+	size_t stage_n = 0;
+	int stage_cap = 0;
+	int nwarps = 0;
+	float* dL = nullptr;
+	size_t dL_n = 0;
+	float* Lx = nullptr;
+	size_t Lx_n = 0;
+	int64_t* leaves = nullptr;
+	size_t leaves_n = 0;
+};
+
+std::vector<std::pair<Ctx*, KickBuffers>> g_kb;
+
+KickBuffers& kbuf(Ctx* c) {
+	for (auto& e : g_kb) {
+		if (e.first == c) {
+			return e.second;
+		}
+	}
+	g_kb.emplace_back(c, KickBuffers());
+	return g_kb.back().second;
+}
+
+template<class T>
+ct_status ensure(Ctx* c, T** p, size_t& have, size_t need, const char* what) {
+	if (need <= have && *p) {
+		return CT_OK;
+	}
+	if (*p) {
+		dfree(c, *p, sizeof(T) * have);
+		*p = nullptr;
+	}
+	const size_t n = std::max(need, have * 3 / 2);
+	CT_TRY(dalloc(c, (void**) p, sizeof(T) * n, what));
+	have = n;
+	return CT_OK;
+}
+
+template<class Ops>
+ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) {
+	cudaStream_t st = c->stream;
+	KickBuffers& K = kbuf(c);
+	const int64_t nn = b->nnodes;
+	const int64_t np = b->n - b->rung_begin;
+	// per-node list descriptors
+	CT_TRY(ensure(c, &K.per_node, K.per_node_n, (size_t) 7 * nn, "walk descriptors"));
+	CT_TRY(ensure(c, &K.dL, K.dL_n, (size_t) NEXP_STRIDE * nn, "expansion deltas"));
+	CT_TRY(ensure(c, &K.Lx, K.Lx_n, (size_t) NEXP_STRIDE * nn, "local expansions"));
+	CT_TRY(ensure(c, &K.leaves, K.leaves_n, (size_t) nn, "leaf index"));
+	K.nwarps = c->nsm * 16 * (WALK_TPB / 32) / 4;  // 4 blocks of 4 warps per SM
+	if (K.stage_cap == 0) {
+		K.stage_cap = 4096;
+	}
+	if (K.cap_cc == 0) {
+		K.cap_cc = std::max<long long>(1 << 20, 256LL * nn);
+		K.cap_leaf = std::max<long long>(1 << 20, 128LL * nn);
+		K.cap_pass = std::max<long long>(1 << 20, 256LL * nn);
+	}
+	double* counters = c->d_counters;
+	for (int attempt = 0; attempt < 6; attempt++) {
+		// (re)allocate list storage at the current capacities
+		CT_TRY(ensure(c, &K.cc, K.cc_n, (size_t) 2 * K.cap_cc, "CC lists"));
+		CT_TRY(ensure(c, &K.leafl, K.leaf_n, (size_t) 3 * K.cap_leaf, "leaf lists"));
+		CT_TRY(ensure(c, &K.pass, K.pass_n, (size_t) 2 * K.cap_pass, "pass-down lists"));
+		CT_TRY(ensure(c, &K.stage, K.stage_n, (size_t) K.nwarps * NLIST * K.stage_cap, "walk staging"));
+		WalkOut o;
+		o.ecc = K.per_node;
+		o.dcc = K.per_node + nn;
+		o.cp = K.per_node + 2 * nn;
+		o.pc = K.per_node + 3 * nn;
+		o.pp = K.per_node + 4 * nn;
+		o.eout = K.per_node + 5 * nn;
+		o.dout = K.per_node + 6 * nn;
+		o.ecc_list = K.cc;
+		o.dcc_list = K.cc + K.cap_cc;
+		o.cp_list = K.leafl;
+		o.pc_list = K.leafl + K.cap_leaf;
+		o.pp_list = K.leafl + 2 * K.cap_leaf;
+		o.cap_cc = K.cap_cc;
+		o.cap_leaf = K.cap_leaf;
+		o.cap_pass = K.cap_pass;  // buffers hold at least 2x / 3x these
+		o.stage = K.stage;
+		o.stage_cap = K.stage_cap;
+		o.flags = c->d_flags;
+		o.cursor = (unsigned long long*) (c->d_flags + 16);
+		CT_CUDA(c, cudaMemsetAsync(c->d_flags, 0, 64 * sizeof(int), st));
+		WalkParams wp;
+		wp.thetainv = 1.f / kp->theta;
+		wp.h = kp->h;
+		cudaEventRecord(c->ev[0], st);
+		const int nlev = (int) b->level_start.size() - 1;
+		for (int k = 0; k < nlev; k++) {
+			const int64_t lb = b->level_start[k], le = b->level_start[k + 1];
+			o.pass_cur = K.pass + (k & 1) * K.cap_pass;
+			o.pass_prev = K.pass + ((k + 1) & 1) * K.cap_pass;
+			// pass-down cursor restarts every level (its buffer alternates)
+			CT_CUDA(c, cudaMemsetAsync(o.cursor + 5, 0, sizeof(unsigned long long), st));
+			const int64_t nwn = std::min<int64_t>((le - lb + 3) / 4, (int64_t) K.nwarps / 4);
+			k_walk<<<(int) std::max<int64_t>(nwn, 1), WALK_TPB, 0, st>>>(lb, le, b->nodes, b->nbox, b->parent, o, wp);
+		}
+		CT_CUDA(c, cudaGetLastError());
+		cudaEventRecord(c->ev[1], st);
+		int* hf = (int*) c->pinned;
+		CT_CUDA(c, cudaMemcpyAsync(hf, c->d_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+		CT_CUDA(c, cudaStreamSynchronize(st));
+		if (hf[1]) {
+			return fail(c, CT_ERR_STATE, "an Ewald check failed the opening test against a leaf; the tree was built with a different theta");
+		}
+		if (hf[0]) {
+			// overflow: grow everything and retry
+			K.stage_cap *= 2;
+			K.cap_cc *= 2;
+			K.cap_leaf *= 2;
+			K.cap_pass *= 2;
+			continue;
+		}
+		// ---- interactions
+		CT_CUDA(c, cudaMemsetAsync(counters, 0, 16 * sizeof(double), st));
+		const int gm = c->nsm * 8;
+		k_m2l_ewald<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL, kp->do_phi, counters);
+		k_m2l_direct<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL, kp->do_phi,
+				counters);
+		cudaEventRecord(c->ev[2], st);
+		for (int k = 0; k < nlev; k++) {
+			const int64_t lb = b->level_start[k], le = b->level_start[k + 1];
+			const int64_t g = (le - lb + 127) / 128;
+			k_l2l<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>(g, c->nsm * 16)), 128, 0, st>>>(lb, le, b->nodes, b->parent, K.dL, K.Lx, kp->do_phi);
+		}
+		cudaEventRecord(c->ev[3], st);
+		// leaves
+		unsigned long long* lcount = (unsigned long long*) (c->d_flags + 40);
+		CT_CUDA(c, cudaMemsetAsync(lcount, 0, sizeof(unsigned long long), st));
+		k_collect_leaves<<<(int) std::max<int64_t>(1, std::min<int64_t>((nn + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nn, b->nodes, K.leaves, lcount);
+		CT_CUDA(c, cudaMemcpyAsync(hf, lcount, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+		CT_CUDA(c, cudaStreamSynchronize(st));
+		const int64_t nleaves = (int64_t) * (unsigned long long*) hf;
+		LeafArgs la;
+		la.nodes = b->nodes;
+		la.multi = b->multi;
+		la.Lx = K.Lx;
+		la.leaves = K.leaves;
+		la.nleaves = nleaves;
+		la.pc = o.pc;
+		la.pc_list = o.pc_list;
+		la.pp = o.pp;
+		la.pp_list = o.pp_list;
+		for (int d = 0; d < 3; d++) {
+			la.x[d] = b->x[d];
+			la.v[d] = b->v[d];
+			la.g[d] = b->g[d];
+		}
+		la.rung = b->rung;
+		la.pot = b->pot;
+		la.kp = *kp;
+		la.compensated = 1;
+		la.sums = counters + 4;
+		la.max_rung = c->d_flags + 48;
+		cudaEventRecord(c->ev[4], st);
+		if (nleaves > 0) {
+			k_leaf<Ops><<<(int) std::min<int64_t>(nleaves, (int64_t) c->nsm * 16), LEAF_TPB, 0, st>>>(la);
+		}
+		cudaEventRecord(c->ev[5], st);
+		CT_CUDA(c, cudaGetLastError());
+		double* hd = (double*) c->pinned;
+		CT_CUDA(c, cudaMemcpyAsync(hd, counters, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
+		CT_CUDA(c, cudaMemcpyAsync(hd + 16, c->d_flags + 48, sizeof(int), cudaMemcpyDeviceToHost, st));
+		unsigned long long* hcur = (unsigned long long*) (hd + 20);
+		CT_CUDA(c, cudaMemcpyAsync(hcur, o.cursor, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+		CT_CUDA(c, cudaStreamSynchronize(st));
+		ct_kick_return r;
+		r.pot = hd[4];
+		r.kin = hd[5];
+		r.dkin = hd[6];
+		r.xmom = hd[7];
+		r.ymom = hd[8];
+		r.zmom = hd[9];
+		r.nmom = hd[10];
+		r.max_rung = *(int*) (hd + 16);
+		if (out) {
+			*out = r;
+		}
+		ct_counters& C = b->counters;
+		C.cc_ewald = (double) hcur[0];
+		C.cc_direct = (double) hcur[1];
+		C.pc_pairs = hd[12];
+		C.pp_pairs = hd[11];
+		C.cp_pairs = hd[1];
+		C.nodes = (double) nn;
+		C.leaves = (double) nleaves;
+		const double icnt = hd[0];
+		const bool phi = kp->do_phi != 0;
+		C.flops_pp = FLOP_PP * C.pp_pairs;
+		// the reference's per-interaction counts (fmm_kernels.hpp:315,724,1486; gravity.cu:62,140,197,343;
+		// kick.cu:153,257)
+		C.flops_cc = C.cc_direct * (6 + FLOP_GREENS + FLOP_M2L + phi * FLOP_M2L_PHI) +
+				C.cc_ewald * (3 + 7 + 140 * 92 + 540 + FLOP_M2L + phi * FLOP_M2L_PHI) + 843.0 * icnt;
+		C.flops = C.flops_pp + C.flops_cc + C.cp_pairs * (Ops::NEXP + 6 + FLOP_GREENS) + C.pc_pairs * (6 + FLOP_GREENS + FLOP_M2L2 + phi * FLOP_M2L_PHI + 4)
+				+ (double) nn * (FLOP_L2L + phi * FLOP_L2L_PHI) + (double) np * (FLOP_KICK + phi * FLOP_KICK_PHI);
+		float ms = 0;
+		cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+		C.ms_walk = ms;
+		cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
+		C.ms_m2l = ms;
+		cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+		C.ms_l2l = ms;
+		cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+		C.ms_leaf = ms;
+		b->have_force = kp->save_force != 0;
+		return CT_OK;
+	}
+	return fail(c, CT_ERR_CAPACITY, "interaction lists overflowed after repeated regrowth");
+}
+
+}  // namespace
+
+ct_status ewald_init(Ctx* c) {
+	cudaStream_t st = c->stream;
+	if (c->order == 5) {
+		static ct_p5::EwaldTab h;
+		ct_p5::ewald_build_indices(h);
+		ct_p5::EwaldTab* d = nullptr;
+		CT_TRY(dalloc(c, (void**) &d, sizeof(h), "Ewald tables"));
+		CT_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+		k_ewald_four5<<<1, 128, 0, st>>>(d);
+		CT_CUDA(c, cudaMemcpyToSymbolAsync(c_tab5, d, sizeof(h), 0, cudaMemcpyDeviceToDevice, st));
+		CT_CUDA(c, cudaStreamSynchronize(st));
+		dfree(c, d, sizeof(h));
+	} else {
+		static ct_p7::EwaldTab h;
+		ct_p7::ewald_build_indices(h);
+		ct_p7::EwaldTab* d = nullptr;
+		CT_TRY(dalloc(c, (void**) &d, sizeof(h), "Ewald tables"));
+		CT_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+		k_ewald_four7<<<1, 128, 0, st>>>(d);
+		CT_CUDA(c, cudaMemcpyToSymbolAsync(c_tab7, d, sizeof(h), 0, cudaMemcpyDeviceToDevice, st));
+		CT_CUDA(c, cudaStreamSynchronize(st));
+		dfree(c, d, sizeof(h));
+	}
+	return CT_OK;
+}
+
+ct_status kick_run(Ctx* c, Box* b, const ct_kick_params* p, ct_kick_return* out) {
+	if (c->order == 5) {
+		return kick_t<Ops5>(c, b, p, out);
+	}
+	return kick_t<Ops7>(c, b, p, out);
+}
+
+}  // namespace ct

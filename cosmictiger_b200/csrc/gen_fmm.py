@@ -528,12 +528,24 @@ def gen_header(P):
     h.append(gen_l2l(P, 2).rstrip())
     h.append("}")
     h.append("")
-    h.append("// Exponents (x,y,z) of the full packed symmetric tensor components, order-major.")
-    h.append("constexpr unsigned char FULL_IDX[NFULL][3] = {%s};" % ", ".join("{%d,%d,%d}" % n for n in sorted(full_set(P), key=sym_index)))
-    h.append("// Exponents (x,y,z) of the stored components of a local expansion, in storage order.")
-    h.append("constexpr unsigned char EXP_IDX[NEXP][3] = {%s};" % ", ".join("{%d,%d,%d}" % n for n in tl_stored(P)))
-    h.append("// Exponents (x,y,z) of the stored components of a multipole, in storage order.")
-    h.append("constexpr unsigned char MULT_IDX[NMULT][3] = {%s};" % ", ".join("{%d,%d,%d}" % n for n in tl_stored(Q)))
+    def table(name, ctype, dims, body, comment):
+        # one host copy and one __constant__ device copy, read through an accessor
+        h.append("// " + comment)
+        h.append("static constexpr %s %s_H%s = {%s};" % (ctype, name, dims, body))
+        h.append("#ifdef __CUDACC__")
+        h.append("static __constant__ %s %s_D%s = {%s};" % (ctype, name, dims, body))
+        h.append("#endif")
+    table("FULL_IDX", "unsigned char", "[NFULL][3]", ", ".join("{%d,%d,%d}" % n for n in sorted(full_set(P), key=sym_index)),
+          "Exponents (x,y,z) of the full packed symmetric tensor components, order-major.")
+    table("EXP_IDX", "unsigned char", "[NEXP][3]", ", ".join("{%d,%d,%d}" % n for n in tl_stored(P)),
+          "Exponents (x,y,z) of the stored components of a local expansion, in storage order.")
+    table("MULT_IDX", "unsigned char", "[NMULT][3]", ", ".join("{%d,%d,%d}" % n for n in tl_stored(Q)),
+          "Exponents (x,y,z) of the stored components of a multipole, in storage order.")
+    h.append("#ifdef __CUDA_ARCH__")
+    h.append("#define CT_TAB(name) name##_D")
+    h.append("#else")
+    h.append("#define CT_TAB(name) name##_H")
+    h.append("#endif")
     h.append("")
     # series of (z^-1 d/dz)^l [erf(z)/z] in w = z^2 (used by ewald_greens for the n = 0 image)
     K = 26
@@ -547,7 +559,11 @@ def gen_header(P):
         rows.append("{" + ", ".join("%.17g" % v for v in row) + "}")
     h.append("// (z^-1 d/dz)^l [erf(z)/z] = sum_j ERF_SERIES[l][j] z^(2j), |z| <= 1.8 (26 terms)")
     h.append("constexpr int ERF_SERIES_N = %d;" % K)
-    h.append("constexpr double ERF_SERIES[ORDER][ERF_SERIES_N] = {%s};" % ",\n\t".join(rows))
+    body = ",\n\t".join(rows)
+    h.append("static constexpr double ERF_SERIES_H[ORDER][ERF_SERIES_N] = {%s};" % body)
+    h.append("#ifdef __CUDACC__")
+    h.append("static __constant__ double ERF_SERIES_D[ORDER][ERF_SERIES_N] = {%s};" % body)
+    h.append("#endif")
     h.append(EWALD_TEMPLATE)
     h.append("}  // namespace %s" % ns)
     return "\n".join(h) + "\n"
@@ -583,9 +599,9 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 			T zl = T(1);
 			T bl = T(2e-3);
 			for (int l = 0; l < ORDER; l++) {
-				T s = T(ERF_SERIES[l][ERF_SERIES_N - 1]);
+				T s = T(CT_TAB(ERF_SERIES)[l][ERF_SERIES_N - 1]);
 				for (int j = ERF_SERIES_N - 2; j >= 0; j--) {
-					s = ct_fma(s, w, T(ERF_SERIES[l][j]));
+					s = ct_fma(s, w, T(CT_TAB(ERF_SERIES)[l][j]));
 				}
 				g[l] = bl * zl * s;
 				zl *= zz;
@@ -629,7 +645,7 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 		T sn, cn;
 		ct_sincos(T(6.2831853071795865e-3) * hdotx, &sn, &cn);
 		for (int k = 0; k < NEXP; k++) {
-			const int order = EXP_IDX[k][0] + EXP_IDX[k][1] + EXP_IDX[k][2];
+			const int order = CT_TAB(EXP_IDX)[k][0] + CT_TAB(EXP_IDX)[k][1] + CT_TAB(EXP_IDX)[k][2];
 			Df[k] = ct_fma((order & 1) ? sn : cn, T(tab.four_exp[i][k]), Df[k]);
 		}
 	}
@@ -658,7 +674,7 @@ CT_HD_FN void ewald_four_entry(double* __restrict__ out, double hx, double hy, d
 	const double sgn[4] = { 1.0, -1.0, -1.0, 1.0 };
 	double F[NFULL];
 	for (int c = 0; c < NFULL; c++) {
-		const int a = FULL_IDX[c][0], b = FULL_IDX[c][1], d = FULL_IDX[c][2];
+		const int a = CT_TAB(FULL_IDX)[c][0], b = CT_TAB(FULL_IDX)[c][1], d = CT_TAB(FULL_IDX)[c][2];
 		const int N = a + b + d;
 		double v = c0 * 1e-3 * sgn[N % 4];
 		for (int k = 0; k < a; k++) v *= hx * w;
@@ -673,7 +689,7 @@ CT_HD_FN void ewald_four_entry(double* __restrict__ out, double hx, double hy, d
 // all-even n: 2 (-2)^k beta^(N+1) / ((N+1) sqrt(pi)) prod (n_i-1)!!, N = 2k, beta = 2e-3
 // (src/ewald_indices.cu:89-101 stores the negative of this).
 CT_HD_FN double ewald_d0_entry(int c) {
-	const int a = FULL_IDX[c][0], b = FULL_IDX[c][1], d = FULL_IDX[c][2];
+	const int a = CT_TAB(FULL_IDX)[c][0], b = CT_TAB(FULL_IDX)[c][1], d = CT_TAB(FULL_IDX)[c][2];
 	if ((a & 1) || (b & 1) || (d & 1)) {
 		return 0.0;
 	}

@@ -1,0 +1,158 @@
+/*
+ * ct_gravity.h — C ABI of the B200 gravity step (tree build, kick, drift).
+ *
+ * Drop-in boundary for the reference's gravity call surface.  Every entry point is
+ * extern "C", takes plain pointers and sizes, returns a ct_status (0 = success, negative
+ * = error; the message is available from ct_last_error) and never throws.  A context owns
+ * one CUDA device, one stream and every box's device-resident state between calls.
+ * Calls on one context must come from one host thread at a time.
+ *
+ * Reference interfaces replaced (paths inside dmarce1/cosmictiger):
+ *   particle store       cosmictiger/particles.hpp:159-171 (particles_x/v/r/g/p globals)
+ *   sort_by_rung         src/particles.cpp:1029-1076  particles_sort_by_rung(int)
+ *   tree_create          cosmictiger/tree.hpp:209-210, src/tree.cpp:273-601
+ *   kick                 cosmictiger/kick.hpp:199-200, src/kick.cpp:150-507,
+ *                        src/kick.cu:179-609 (cuda_execute_kicks)
+ *   drift                cosmictiger/drift.hpp:51-54, src/drift.cu:36-185
+ *   ewald_const::init    cosmictiger/ewald_indices.hpp:32-41, src/ewald_indices.cu:30-114
+ */
+#ifndef CT_GRAVITY_H
+#define CT_GRAVITY_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int ct_status;
+#define CT_OK 0
+#define CT_ERR_ARG -1        /* invalid argument */
+#define CT_ERR_CUDA -2       /* a CUDA runtime call failed */
+#define CT_ERR_MEMORY -3     /* device memory or HBM budget exhausted */
+#define CT_ERR_CAPACITY -4   /* an internal list overflowed even after regrowth */
+#define CT_ERR_STATE -5      /* call out of order (e.g. kick before tree_create) */
+
+typedef struct ct_ctx ct_ctx;
+
+/* Mirror of kick_params (cosmictiger/kick.hpp:138-186); field meaning is the reference's.
+ * min_level, gpu, node_load and vel_init have no role on a single device and are absent. */
+typedef struct {
+	float sign;       /* +1, or -1 for glass creation */
+	int min_rung;     /* rung being kicked */
+	float a;          /* scale factor */
+	float t0;         /* top-level time step */
+	float theta;      /* opening angle */
+	float h;          /* softening kernel support (box units) */
+	float eta;        /* time-step criterion */
+	float GM;         /* gravitational constant times particle mass */
+	float max_dt;     /* cap on a particle's time step */
+	int save_force;   /* keep g and phi per particle */
+	int first_call;   /* first kick of a run: no ascending half kick */
+	int ascending;    /* apply the ascending half kick */
+	int descending;   /* assign rungs and apply the descending half kick */
+	int top;          /* top of the rung ladder */
+	int do_phi;       /* compute potentials */
+} ct_kick_params;
+
+/* Mirror of kick_return (cosmictiger/kick.hpp:92-136). */
+typedef struct {
+	int max_rung;
+	double pot;
+	double kin;
+	double dkin;
+	double xmom;
+	double ymom;
+	double zmom;
+	double nmom;
+} ct_kick_return;
+
+/* Tree-construction parameters (tree_create_params, cosmictiger/tree.hpp:186-207, plus the
+ * option values tree_create reads: bucket_size and hsoft, src/options.cpp:107,165,217). */
+typedef struct {
+	int min_rung;     /* tree over particles with rung >= min_rung, i.e. [rung_begin, n) */
+	double theta;
+	double hsoft;     /* softening support h, box units */
+	int bucket;       /* leaf capacity (reference default 128) */
+} ct_tree_params;
+
+/* A tree node as exported for inspection (the reference's tree_node, tree.hpp:98-169,
+ * plus its heap key).  Order of export: breadth-first. */
+typedef struct {
+	uint64_t key;            /* heap key: root 1, children 2k and 2k+1 */
+	int32_t part_begin, part_end;
+	int32_t child_left, child_right; /* export indices, -1 for leaves */
+	uint32_t pos[3];         /* expansion centre, fixed32 */
+	float radius;
+	int32_t box_begin[3], box_end[3]; /* tight box, fixed<int,29> raw */
+	int32_t leaf;
+	int32_t depth;
+	float multi[37];         /* multipole (first (order-1)^2+1 used) */
+} ct_node;
+
+/* Counters of the last kick (interactions by kind and the reference's flop convention). */
+typedef struct {
+	double pp_pairs;      /* particle-particle pairs */
+	double cc_direct;     /* M2L, direct Green's function */
+	double cc_ewald;      /* M2L, Ewald Green's function */
+	double cp_pairs;      /* P2L (particle -> local expansion) */
+	double pc_pairs;      /* M2P (multipole -> particle) */
+	double nodes;
+	double leaves;
+	double flops;         /* total, per the reference's per-interaction counts */
+	double flops_pp;
+	double flops_cc;
+	double ms_tree, ms_walk, ms_m2l, ms_l2l, ms_leaf, ms_drift; /* device time of the last calls */
+} ct_counters;
+
+/* ---- context */
+ct_status ct_ctx_create(ct_ctx** out, int device, size_t hbm_budget_bytes, int order);
+void ct_ctx_destroy(ct_ctx* ctx);
+const char* ct_last_error(const ct_ctx* ctx);
+int ct_order(const ct_ctx* ctx);
+
+/* ---- boxes (independent periodic unit boxes with their own particles and tree) */
+ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id);
+ct_status ct_box_destroy(ct_ctx* ctx, int box_id);
+int64_t ct_box_size(const ct_ctx* ctx, int box_id);
+
+/* Host <-> device transfers.  x,y,z: fixed32 positions (uint32, 2^-32 box units);
+ * vxyz: float[3*n] interleaved velocities (the reference's particles_v layout);
+ * rung: int8[n].  Download arguments may be NULL to skip a field; g/pot only exist after a
+ * kick with save_force. */
+ct_status ct_box_upload(ct_ctx* ctx, int box_id, const uint32_t* x, const uint32_t* y, const uint32_t* z, const float* vxyz, const int8_t* rung);
+ct_status ct_box_download(ct_ctx* ctx, int box_id, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy,
+		float* gz, float* pot);
+
+/* Device-pointer variants (same layout, memory on the context's device). */
+ct_status ct_box_upload_device(ct_ctx* ctx, int box_id, const uint32_t* x, const uint32_t* y, const uint32_t* z, const float* vxyz,
+		const int8_t* rung);
+ct_status ct_box_download_device(ct_ctx* ctx, int box_id, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, float* gx,
+		float* gy, float* gz, float* pot);
+
+/* ---- the gravity step (particles_sort_by_rung, tree_create, kick, drift) */
+ct_status ct_sort_by_rung(ct_ctx* ctx, int box_id, int min_rung, int64_t* rung_begin);
+ct_status ct_tree_create(ct_ctx* ctx, int box_id, const ct_tree_params* params, int64_t* node_count);
+ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* result);
+ct_status ct_drift(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag);
+
+/* Tree export (breadth-first order) for inspection and parity checks. */
+ct_status ct_tree_download(ct_ctx* ctx, int box_id, ct_node* nodes, int64_t max_nodes, int64_t* count);
+
+/* Counters of the last tree/kick/drift on a box. */
+ct_status ct_get_counters(ct_ctx* ctx, int box_id, ct_counters* out);
+
+/* Wait for all work of the context. */
+ct_status ct_synchronize(ct_ctx* ctx);
+
+/* FP64 direct Ewald summation (accuracy reference, not part of the step): force and
+ * potential of all box particles (unit mass each) on nsink sink positions, softened nearest
+ * image plus the periodic correction, alpha = 2.  Results in double, unscaled by GM. */
+ct_status ct_direct_ewald(ct_ctx* ctx, int box_id, int64_t nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, double h, double* gx,
+		double* gy, double* gz, double* pot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
