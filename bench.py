@@ -1,0 +1,400 @@
+#!/usr/bin/env python3
+"""Gravity-step benchmark: particle-steps/s of tree build + kick + drift on one B200.
+
+Workload (default): the clustered 256^3 box -- 70% of 16.8M particles on a Zel'dovich-displaced
+lattice (P(k) ~ k^-1.5, 0.5 mean-spacing RMS), 30% in 20,000 Plummer spheres with power-law
+masses -- at theta = 0.55, expansion order 7, softening 1/50 of the mean spacing, Ewald on.
+A step is one tree build over all particles, one kick (forces, velocities, rungs) and one
+drift.  Inputs are seeded synthetic stand-ins generated here (no dataset is involved).
+
+  value   particle-steps/s with particles resident in HBM (device-timed, CUDA events)
+  e2e     the same through the public API with host buffers: every step uploads the
+          particles from pinned host memory and downloads positions, velocities and rungs
+  roofline  the leaf kernel (P2P + M2P + L2P + kick, the dominant kernel) against the measured
+          FP32 FMA peak, flops counted with the reference's per-interaction convention
+  cpu_baseline  the CPU oracle (this project's restatement of the reference's algorithm; the
+          reference's own CPU kick cannot run) on a bounded sample of the same workload
+
+--impl reference times that CPU implementation alone on all host cores.
+Multi-GPU (--gpus N under torchrun): independent boxes per rank (weak scaling, no collective
+on the data path); value = all ranks' particle-steps / max rank time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="particles = n^3")
+    ap.add_argument("--theta", type=float, default=0.55)
+    ap.add_argument("--workload", default="clustered", choices=["clustered", "lattice"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--accuracy-sinks", type=int, default=0, help="FP64 direct-Ewald check on this many sinks (0: skip)")
+    return ap.parse_args()
+
+
+def make_ics(args, seed):
+    from cosmictiger_b200 import ics
+
+    if args.workload == "clustered":
+        nsph = max(1, int(round(20000 * (args.n / 256.0) ** 3)))
+        return ics.clustered_box(args.n, nspheres=nsph, seed=seed)
+    return ics.zeldovich_lattice(args.n, index=-2.0, rms_spacing=0.25, seed=seed)
+
+
+def workload_name(args):
+    if args.workload == "clustered":
+        return "clustered %d^3 (70%% Zel'dovich k^-1.5 / 30%% Plummer), theta %.2f, order 7, Ewald, all particles per step" % (args.n, args.theta)
+    return "lattice %d^3 Zel'dovich k^-2, theta %.2f, order 7, Ewald, all particles per step" % (args.n, args.theta)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [s.strip() for s in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import ics
+
+    x, y, z, v, r = make_ics(args, seed=3 + 101 * rank)
+    N = len(x)
+    theta = args.theta
+    h = ics.softening(N, 0.02)
+    GM = 1.0 / N
+    eta = ics.eta_default()
+    t0 = 1.0 / 64
+    ctx = ct.Context(device=local, order=7)
+    box = ctx.box(N)
+    box.upload(x, y, z, v, r)
+
+    def step(first):
+        box.tree_create(theta, h, 128)
+        kp = ct.KickParams.make(theta=theta, h=h, GM=GM, eta=eta, t0=t0, first_call=first, save_force=False)
+        kr = box.kick(kp)
+        box.drift(0, 1.0, t0)
+        return kr
+
+    # warm-up (the first is the reference's first call: no ascending half kick)
+    for i in range(args.warmup):
+        step(i == 0)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    # events on the library's own stream
+    ctx.lib.ct_stream.argtypes = [ctypes.c_void_p]
+    ctx.lib.ct_stream.restype = ctypes.c_void_p
+    lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    launches0 = ctx.launches()
+    t_start = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(lib_stream)
+    leaf_ms = []
+    walk_ms, m2l_ms, tree_ms = [], [], []
+    counters = None
+    for i in range(args.steps):
+        step(False)
+        c = box.counters()
+        leaf_ms.append(c["ms_leaf"])
+        walk_ms.append(c["ms_walk"])
+        m2l_ms.append(c["ms_m2l"])
+        tree_ms.append(c["ms_tree"])
+        counters = c
+    ev1.record(lib_stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t_start
+    launches = ctx.launches() - launches0
+    clocks = sampler.stop()
+    ms_dev = ev0.elapsed_time(ev1)
+    ms_step = ms_dev / args.steps
+    t_max = ms_dev
+    if pg:
+        tt = torch.tensor([ms_dev], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = N * world * args.steps / (t_max / 1e3)
+    # ---- e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        hx, hy, hz = (torch.from_numpy(a.copy()).pin_memory().numpy() for a in (x, y, z))
+        hv = torch.from_numpy(v.copy()).pin_memory().numpy()
+        hr = torch.from_numpy(r.copy()).pin_memory().numpy()
+        ox, oy, oz = (torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32) for _ in range(3))
+        ov = torch.empty((N, 3), dtype=torch.float32).pin_memory().numpy()
+        orr = torch.empty(N, dtype=torch.int8).pin_memory().numpy()
+        import ctypes
+
+        def e2e_step(first):
+            box.upload(hx, hy, hz, hv, hr)
+            step(first)
+            p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+            ctx.check(ctx.lib.ct_box_download(ctx.h, box.id, p(ox), p(oy), p(oz), p(ov), p(orr), None, None, None, None), "download")
+
+        e2e_step(True)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        ke = max(1, min(args.steps, 3))
+        for i in range(ke):
+            e2e_step(False)
+        e1.record(lib_stream)
+        torch.cuda.synchronize()
+        ms_e = e0.elapsed_time(e1)
+        if pg:
+            tt = torch.tensor([ms_e], device="cuda")
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            ms_e = float(tt.item())
+        e2e = {"value": N * world * ke / (ms_e / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(N * (12 + 12 + 1)),
+               "d2h_bytes_per_step": int(N * (12 + 12 + 1))}
+    # ---- roofline of the leaf kernel (reference flop convention)
+    import ctypes
+
+    L = ctx.lib
+    L.ct_fp32_peak.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    pk = ctypes.c_double(0)
+    ctx.check(L.ct_fp32_peak(ctx.h, ctypes.byref(pk)), "ct_fp32_peak")
+    peak_tf = pk.value
+    c = counters
+    npart = N
+    leaf_flops = 21.0 * c["pp_pairs"] + c["pc_pairs"] * (6 + 265 + 520 + 119 + 4) + npart * (557 + 178)
+    leaf_s = float(np.mean(leaf_ms)) / 1e3
+    achieved = leaf_flops / leaf_s / 1e12
+    traffic = read_traffic()
+    roofline = {"bound": "fp32_fma", "kernel": "k_leaf (P2P+M2P+L2P+kick)", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+                "frac": achieved / peak_tf if peak_tf else None, "traffic": traffic,
+                "peak_source": "measured on this GPU by ct_fp32_peak (FMA chain, 2 flops per FMA); MEASURED_PEAKS.json has no FP32 entry"}
+    extra = {"ms_tree": float(np.mean(tree_ms)), "ms_walk": float(np.mean(walk_ms)), "ms_m2l": float(np.mean(m2l_ms)), "ms_leaf": float(np.mean(leaf_ms)),
+             "pp_pairs": c["pp_pairs"], "cc_direct": c["cc_direct"], "cc_ewald": c["cc_ewald"], "pc_pairs": c["pc_pairs"], "cp_pairs": c["cp_pairs"],
+             "nodes": c["nodes"], "leaves": c["leaves"], "flops_per_step": c["flops"], "wall_s": wall}
+    acc = None
+    if args.accuracy_sinks and rank == 0:
+        acc = accuracy(box, args.accuracy_sinks, h, N)
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        cpu = cpu_baseline(args)
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s at <=1e-3 rms force err; ensemble-batched vs plain; p50/p99 ms",
+            "value": value,
+            "unit": "particle-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (fixed32 positions, f64 tree geometry)",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": workload_name(args), "particles_per_gpu": N, "theta": theta, "order": 7, "bucket": 128,
+                       "parallelism": "independent boxes per GPU" if world > 1 else "single box",
+                       "l2": "inputs larger than L2 (%.0f MB of particle state)" % (N * 41 / 1e6)},
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "breakdown": extra,
+        }
+        if acc:
+            line["force_error"] = acc
+        print(json.dumps(line), flush=True)
+    box.close()
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def read_traffic():
+    """DRAM bytes per launch of the leaf kernel from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "k_leaf_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    try:
+        for ln in open(p):
+            if ln.startswith("dram_bytes_per_launch_full_size="):
+                return float(ln.split("=", 1)[1])
+    except Exception:
+        return None
+    return None
+
+
+def accuracy(box, nsink, h, N):
+    """Force error of the last kick vs the FP64 direct Ewald sum on nsink seeded sinks."""
+    import cosmictiger_b200 as ct
+
+    st = box.download(forces=False)
+    rng = np.random.default_rng(4321 + 42)
+    sel = np.sort(rng.choice(N, size=min(nsink, N), replace=False))
+    # recompute forces at the current positions (a kick with save_force)
+    box.tree_create(box.tree_params.theta, h, 128)
+    kp = ct.KickParams.make(theta=box.tree_params.theta, h=h, GM=1.0 / N, eta=0.25 / np.sqrt(693 / 256.0), save_force=True, descending=False,
+                            ascending=False)
+    box.kick(kp)
+    out = box.download(forces=True)
+    dg = box.direct_ewald(out["x"][sel], out["y"][sel], out["z"][sel], h)
+    gt = np.stack([out["gx"][sel], out["gy"][sel], out["gz"][sel]], 1).astype(np.float64)
+    gd = np.stack(dg[:3], 1) / N
+    err = np.linalg.norm(gt - gd, axis=1) / np.linalg.norm(gd, axis=1)
+    mag = np.abs(np.linalg.norm(gt, axis=1) - np.linalg.norm(gd, axis=1)) / np.linalg.norm(gd, axis=1)
+    del st
+    return {"sinks": int(len(sel)), "rms_rel": float(np.sqrt(np.mean(err ** 2))), "p99_rel": float(np.percentile(err, 99)),
+            "rms_norm": float(np.sqrt(np.sum((gt - gd) ** 2) / np.sum(gd ** 2))), "mag_p50": float(np.percentile(mag, 50)),
+            "mag_p99": float(np.percentile(mag, 99))}
+
+
+def cpu_measure(args, target_s=12.0, state=None):
+    """Time the CPU oracle on a bounded sample: full tree build and drift, the kick on every
+    k-th top-level work item (k chosen so the kick sample takes about target_s)."""
+    from cosmictiger_b200 import ics
+    from tests import oracle_lib
+
+    O = oracle_lib.load(build=False)
+    if state is None:
+        state = make_ics(args, seed=3)
+    x, y, z, v, r = (a.copy() for a in state)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    t = time.perf_counter()
+    nodes = O.tree_build(x, y, z, v, r, args.theta, h, 128)
+    t_tree = time.perf_counter() - t
+    kp = oracle_lib.KickParams(sign=1.0, min_rung=0, a=1.0, t0=1.0 / 64, theta=args.theta, h=h, eta=ics.eta_default(), GM=1.0 / N, max_dt=1e30,
+                               save_force=1, first_call=0, ascending=1, descending=1, top=1, do_phi=1)
+    ncores = os.cpu_count() or 1
+    # probe with a sparse sample, then size the real sample
+    stride = 4096
+    dt, got, _ = O.kick_sampled(kp, nodes, x, y, z, v.copy(), r.copy(), stride, nthreads=ncores)
+    rate = got / max(dt, 1e-6)
+    want = max(1, int(rate * target_s))
+    stride = max(1, int(round(N / max(want, 1))))
+    dt, got, _ = O.kick_sampled(kp, nodes, x, y, z, v.copy(), r.copy(), stride, nthreads=ncores)
+    t = time.perf_counter()
+    O.drift(x, y, z, v, r, 0, 1.0, 1.0 / 64)
+    t_drift = time.perf_counter() - t
+    t_step = t_tree + dt * (N / max(got, 1)) + t_drift
+    return {"value": N / t_step, "unit": "particle-steps/s", "cores": ncores, "kind": "port",
+            "sample": "%s: full tree build (%.1f s, 1 thread) + drift, kick on every %d-th top-level work item (%d of %d particles, %.1f s, %d threads), "
+                      "kick time scaled to all particles" % (workload_name(args), t_tree, stride, got, N, dt, ncores)}
+
+
+def cpu_baseline(args):
+    try:
+        return cpu_measure(args)
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": "particle-steps/s", "cores": os.cpu_count(), "kind": "port", "sample": "failed: %s" % e}
+
+
+def run_reference(args):
+    """The reference arm: the CPU implementation of the path on all host cores (the oracle port;
+    the reference's own CPU kick aborts in P2P, src/gravity.cpp:257-258)."""
+    vals = []
+    info = None
+    state = make_ics(args, seed=3)
+    for i in range(args.warmup + args.steps):
+        m = cpu_measure(args, target_s=max(2.0, 20.0 / max(1, args.steps)), state=state)
+        if i >= args.warmup:
+            vals.append(m["value"])
+            info = m
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": "particle-steps/s at <=1e-3 rms force err; ensemble-batched vs plain; p50/p99 ms", "value": v,
+            "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * (args.n ** 3) / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": workload_name(args), "theta": args.theta, "order": 7, "bucket": 128, "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": info["cores"], "kind": "port", "sample": info["sample"]},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

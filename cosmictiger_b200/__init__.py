@@ -135,6 +135,8 @@ def library():
     L.ct_tree_download.argtypes = [vp, i32, vp, i64, ctypes.POINTER(i64)]
     L.ct_get_counters.argtypes = [vp, i32, ctypes.POINTER(Counters)]
     L.ct_synchronize.argtypes = [vp]
+    L.ct_launch_count.argtypes = [vp]
+    L.ct_launch_count.restype = ctypes.c_ulonglong
     L.ct_direct_ewald.argtypes = [vp, i32, i64, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
     _lib = L
     return L
@@ -162,6 +164,10 @@ class Context:
 
     def box(self, n):
         return Box(self, n)
+
+    def launches(self):
+        """Kernels of libct_gravity launched on this context so far."""
+        return int(self.lib.ct_launch_count(self.h))
 
     def synchronize(self):
         self.check(self.lib.ct_synchronize(self.h), "ct_synchronize")

@@ -338,6 +338,29 @@ __global__ void k_direct_ewald_four(int nsink, const uint32_t* sx, const uint32_
 	out[4 * s + 3] += phi;
 }
 
+// FP32 FMA throughput probe: 16 independent FMA chains per thread in registers.
+__global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float b, float c) {
+	float a[16];
+#pragma unroll
+	for (int k = 0; k < 16; k++) {
+		a[k] = threadIdx.x * 1e-3f + k;
+	}
+	for (int i = 0; i < iters; i++) {
+#pragma unroll
+		for (int k = 0; k < 16; k++) {
+			a[k] = fmaf(a[k], b, c);
+		}
+	}
+	float s = 0.f;
+#pragma unroll
+	for (int k = 0; k < 16; k++) {
+		s += a[k];
+	}
+	if (s == 1234.5f) {
+		out[threadIdx.x] = s;
+	}
+}
+
 }  // namespace
 
 ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag) {
@@ -346,6 +369,7 @@ ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag) {
 	const int64_t np = b->n - b->rung_begin;
 	cudaEventRecord(c->ev[6], c->stream);
 	if (np > 0) {
+		c->launches++;
 		k_drift<<<grid(c, np, 256), 256, 0, c->stream>>>(b->rung_begin, b->n, b->x[0], b->x[1], b->x[2], b->v[0], b->v[1], b->v[2], b->rung, rung, c1, c0,
 				drag != 0.0);
 	}
@@ -382,14 +406,18 @@ ct_status sort_by_rung_run(Ctx* c, Box* b, int minrung) {
 	void* tmp = scratch(c, 29, std::max(need, need2) + 256, &s);
 	CT_TRY(s);
 	need = std::max(need, need2);
+	c->launches++;
 	k_rung_flags<<<grid(c, n, 256), 256, 0, st>>>(beg, e, b->rung, minrung, lt);
 	CT_CUDA(c, cub::DeviceReduce::Sum(tmp, need, lt, tot, (int) n, st));
+	c->launches++;
 	k_rung_mis<<<grid(c, n, 256), 256, 0, st>>>(beg, e, lt, tot, misL, misR);
 	CT_CUDA(c, cub::DeviceScan::ExclusiveSum(tmp, need, misL, exL, (int) n, st));
 	CT_CUDA(c, cub::DeviceReduce::Sum(tmp, need, misL, tot + 1, (int) n, st));
 	CT_CUDA(c, cub::DeviceScan::ExclusiveSum(tmp, need, misR, exR, (int) n, st));
 	CT_CUDA(c, cub::DeviceReduce::Sum(tmp, need, misR, tot + 2, (int) n, st));
+	c->launches++;
 	k_rung_pos<<<grid(c, n, 256), 256, 0, st>>>(beg, e, misL, misR, exL, exR, tot + 2, posL, posR);
+	c->launches++;
 	k_rung_swap<<<grid(c, n, 256), 256, 0, st>>>(posL, posR, tot + 1, b->x[0], b->x[1], b->x[2], b->v[0], b->v[1], b->v[2], b->rung);
 	int* h = (int*) c->pinned;
 	CT_CUDA(c, cudaMemcpyAsync(h, tot, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -419,11 +447,14 @@ ct_status direct_ewald_run(Ctx* c, Box* b, int64_t nsink, const uint32_t* sx, co
 	CT_CUDA(c, cudaMemsetAsync(CS, 0, 2 * CT_EWALD_NFOUR * sizeof(double), st));
 	const int64_t n = b->n;
 	dim3 gsf((unsigned) std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 64)), CT_EWALD_NFOUR);
+	c->launches++;
 	k_struct_factor<<<gsf, 256, 0, st>>>(n, b->x[0], b->x[1], b->x[2], dfour, CS);
 	for (int64_t s0 = 0; s0 < nsink; s0 += 65535) {
 		const int ns = (int) std::min<int64_t>(65535, nsink - s0);
+		c->launches++;
 		k_direct_ewald<<<ns, 256, 0, st>>>(n, b->x[0], b->x[1], b->x[2], dsk + s0, dsk + nsink + s0, dsk + 2 * nsink + s0, h, dreal, dout + 4 * s0);
 	}
+	c->launches++;
 	k_direct_ewald_four<<<(int) ((nsink + 127) / 128), 128, 0, st>>>((int) nsink, dsk, dsk + nsink, dsk + 2 * nsink, dfour, CS, h, dout);
 	CT_CUDA(c, cudaGetLastError());
 	std::vector<double> hout(4 * nsink);
@@ -522,6 +553,10 @@ void ct_ctx_destroy(ct_ctx* ctx) {
 const char* ct_last_error(const ct_ctx* ctx) {
 	const Ctx* c = (const Ctx*) ctx;
 	return c ? c->err.c_str() : "no context";
+}
+
+unsigned long long ct_launch_count(const ct_ctx* ctx) {
+	return ctx ? ((const Ctx*) ctx)->launches : 0;
 }
 
 int ct_order(const ct_ctx* ctx) {
@@ -623,6 +658,7 @@ static ct_status upload_impl(Ctx* c, Box* b, const uint32_t* x, const uint32_t* 
 		float* tmp = (float*) scratch(c, 33, sizeof(float) * 3 * n, &s);
 		CT_TRY(s);
 		CT_CUDA(c, cudaMemcpyAsync(tmp, vxyz, sizeof(float) * 3 * n, kind, st));
+		c->launches++;
 		k_aos_to_soa<<<grid(c, n, 256), 256, 0, st>>>(n, tmp, b->v[0], b->v[1], b->v[2]);
 	}
 	if (rung) {
@@ -648,6 +684,7 @@ static ct_status download_impl(Ctx* c, Box* b, uint32_t* x, uint32_t* y, uint32_
 		ct_status s = CT_OK;
 		float* tmp = (float*) scratch(c, 33, sizeof(float) * 3 * n, &s);
 		CT_TRY(s);
+		c->launches++;
 		k_soa_to_aos<<<grid(c, n, 256), 256, 0, st>>>(n, b->v[0], b->v[1], b->v[2], tmp);
 		CT_CUDA(c, cudaMemcpyAsync(vxyz, tmp, sizeof(float) * 3 * n, kind, st));
 	}
@@ -855,6 +892,38 @@ ct_status ct_synchronize(ct_ctx* ctx) {
 	}
 	CT_CUDA(c, cudaStreamSynchronize(c->stream));
 	return CT_OK;
+}
+
+ct_status ct_fp32_peak(ct_ctx* ctx, double* tflops) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c || !tflops) {
+		return CT_ERR_ARG;
+	}
+	cudaSetDevice(c->device);
+	ct_status s = CT_OK;
+	float* out = (float*) scratch(c, 34, 1024 * sizeof(float), &s);
+	CT_TRY(s);
+	const int blocks = c->nsm * 8, iters = 8192;
+	double best = 0.0;
+	for (int rep = 0; rep < 4; rep++) {
+		cudaEventRecord(c->ev[10], c->stream);
+		c->launches++;
+		k_fma_peak<<<blocks, 256, 0, c->stream>>>(out, iters, 0.9999999f, 1e-7f);
+		cudaEventRecord(c->ev[11], c->stream);
+		CT_CUDA(c, cudaEventSynchronize(c->ev[11]));
+		float ms = 0.f;
+		cudaEventElapsedTime(&ms, c->ev[10], c->ev[11]);
+		const double fl = 2.0 * 16.0 * iters * 256.0 * blocks;
+		if (rep > 0) {
+			best = std::max(best, fl / (ms * 1e-3) / 1e12);
+		}
+	}
+	*tflops = best;
+	return CT_OK;
+}
+
+void* ct_stream(ct_ctx* ctx) {
+	return ctx ? (void*) ((Ctx*) ctx)->stream : nullptr;
 }
 
 ct_status ct_direct_ewald(ct_ctx* ctx, int box_id, int64_t nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, double h, double* gx,

@@ -108,6 +108,7 @@ struct Ctx {
 	double* d_counters = nullptr; // interaction counters
 	void* d_ewald_tab = nullptr;  // device copy of the Ewald tables (when not in __constant__)
 	cudaEvent_t ev[16];
+	unsigned long long launches = 0;  // kernels of this library launched so far
 };
 
 // Allocation with budget accounting.

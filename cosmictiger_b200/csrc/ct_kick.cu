@@ -946,6 +946,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			// pass-down cursor restarts every level (its buffer alternates)
 			CT_CUDA(c, cudaMemsetAsync(o.cursor + 5, 0, sizeof(unsigned long long), st));
 			const int64_t nwn = std::min<int64_t>((le - lb + 3) / 4, (int64_t) K.nwarps / 4);
+			c->launches++;
 			k_walk<<<(int) std::max<int64_t>(nwn, 1), WALK_TPB, 0, st>>>(lb, le, b->nodes, b->nbox, b->parent, o, wp);
 		}
 		CT_CUDA(c, cudaGetLastError());
@@ -967,19 +968,23 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		// ---- interactions
 		CT_CUDA(c, cudaMemsetAsync(counters, 0, 16 * sizeof(double), st));
 		const int gm = c->nsm * 8;
+		c->launches++;
 		k_m2l_ewald<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL, kp->do_phi, counters);
+		c->launches++;
 		k_m2l_direct<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL, kp->do_phi,
 				counters);
 		cudaEventRecord(c->ev[2], st);
 		for (int k = 0; k < nlev; k++) {
 			const int64_t lb = b->level_start[k], le = b->level_start[k + 1];
 			const int64_t g = (le - lb + 127) / 128;
+			c->launches++;
 			k_l2l<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>(g, c->nsm * 16)), 128, 0, st>>>(lb, le, b->nodes, b->parent, K.dL, K.Lx, kp->do_phi);
 		}
 		cudaEventRecord(c->ev[3], st);
 		// leaves
 		unsigned long long* lcount = (unsigned long long*) (c->d_flags + 40);
 		CT_CUDA(c, cudaMemsetAsync(lcount, 0, sizeof(unsigned long long), st));
+		c->launches++;
 		k_collect_leaves<<<(int) std::max<int64_t>(1, std::min<int64_t>((nn + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nn, b->nodes, K.leaves, lcount);
 		CT_CUDA(c, cudaMemcpyAsync(hf, lcount, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
 		CT_CUDA(c, cudaStreamSynchronize(st));
@@ -1007,6 +1012,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		la.max_rung = c->d_flags + 48;
 		cudaEventRecord(c->ev[4], st);
 		if (nleaves > 0) {
+			c->launches++;
 			k_leaf<Ops><<<(int) std::min<int64_t>(nleaves, (int64_t) c->nsm * 16), LEAF_TPB, 0, st>>>(la);
 		}
 		cudaEventRecord(c->ev[5], st);
@@ -1071,6 +1077,7 @@ ct_status ewald_init(Ctx* c) {
 		ct_p5::EwaldTab* d = nullptr;
 		CT_TRY(dalloc(c, (void**) &d, sizeof(h), "Ewald tables"));
 		CT_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+		c->launches++;
 		k_ewald_four5<<<1, 128, 0, st>>>(d);
 		CT_CUDA(c, cudaMemcpyToSymbolAsync(c_tab5, d, sizeof(h), 0, cudaMemcpyDeviceToDevice, st));
 		CT_CUDA(c, cudaStreamSynchronize(st));
@@ -1081,6 +1088,7 @@ ct_status ewald_init(Ctx* c) {
 		ct_p7::EwaldTab* d = nullptr;
 		CT_TRY(dalloc(c, (void**) &d, sizeof(h), "Ewald tables"));
 		CT_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+		c->launches++;
 		k_ewald_four7<<<1, 128, 0, st>>>(d);
 		CT_CUDA(c, cudaMemcpyToSymbolAsync(c_tab7, d, sizeof(h), 0, cudaMemcpyDeviceToDevice, st));
 		CT_CUDA(c, cudaStreamSynchronize(st));

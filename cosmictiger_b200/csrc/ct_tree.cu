@@ -779,7 +779,9 @@ ct_status tree_build_t(Ctx* c, Box* b, const ct_tree_params* p) {
 	s.posR = (int32_t*) scratch(c, 2, sizeof(int32_t) * n, &s1);
 	CT_TRY(s1);
 	(void) npad;
+	c->launches++;
 	k_iota<<<grid_for(c, n, 256), 256, 0, st>>>(s.idx, n);
+	c->launches++;
 	k_init_root<<<1, 1, 0, st>>>(b->nodes, b->gbox, b->key, b->depth, b->parent, (int32_t) pb, (int32_t) n);
 	CT_CUDA(c, cudaMemsetAsync(c->d_flags, 0, 4 * sizeof(int), st));
 	std::vector<int64_t> levels;
@@ -811,6 +813,7 @@ ct_status tree_build_t(Ctx* c, Box* b, const ct_tree_params* p) {
 		s.cub_bytes = need;
 		s.cub_tmp = scratch(c, 16, need + 256, &s1);
 		CT_TRY(s1);
+		c->launches++;
 		k_classify<<<grid_for(c, nl, 256), 256, 0, st>>>(lb, nl, b->nodes, b->gbox, b->depth, p->theta, p->hsoft, p->bucket, s, c->d_flags);
 		CT_CUDA(c, cudaMemsetAsync(s.split + nl, 0, sizeof(int32_t), st));
 		CT_CUDA(c, cudaMemsetAsync(s.ntiles + nl, 0, sizeof(int32_t), st));
@@ -823,13 +826,19 @@ ct_status tree_build_t(Ctx* c, Box* b, const ct_tree_params* p) {
 		const int ntile = h_tot[1];
 		if (nsplit > 0) {
 			CT_TRY(ensure_nodes(c, b, le + 2 * (int64_t) nsplit));
+			c->launches++;
 			k_tile_map<<<grid_for(c, (int64_t) nl * 32, 256), 256, 0, st>>>(nl, s);
 			const int gt = std::min(ntile, c->nsm * 16);
+			c->launches++;
 			k_count<<<gt, TPB, 0, st>>>(lb, ntile, b->nodes, b->x[0], b->x[1], b->x[2], s);
+			c->launches++;
 			k_node_scan<<<std::min(nl, c->nsm * 16), TPB, 0, st>>>(lb, nl, b->nodes, b->x[0], b->x[1], b->x[2], s);
+			c->launches++;
 			k_positions<<<gt, TPB, 0, st>>>(lb, ntile, b->nodes, b->x[0], b->x[1], b->x[2], s);
+			c->launches++;
 			k_swap<<<gt, TPB, 0, st>>>(lb, ntile, b->nodes, b->x[0], b->x[1], b->x[2], s);
 		}
+		c->launches++;
 		k_children<<<grid_for(c, nl, 256), 256, 0, st>>>(lb, nl, le, b->nodes, b->gbox, b->key, b->depth, b->parent, s);
 		CT_CUDA(c, cudaGetLastError());
 		lb = le;
@@ -850,6 +859,7 @@ ct_status tree_build_t(Ctx* c, Box* b, const ct_tree_params* p) {
 		CT_CUDA(c, cudaMemcpyAsync(t2 + pb, b->v[2] + pb, sizeof(float) * np, cudaMemcpyDeviceToDevice, st));
 		CT_CUDA(c, cudaMemcpyAsync(tr + pb, b->rung + pb, np, cudaMemcpyDeviceToDevice, st));
 		if (np > 0) {
+			c->launches++;
 			k_gather_particles<<<grid_for(c, np, 256), 256, 0, st>>>(pb, n, s.idx, t0, t1, t2, tr, b->v[0], b->v[1], b->v[2], b->rung);
 		}
 	}
@@ -857,6 +867,7 @@ ct_status tree_build_t(Ctx* c, Box* b, const ct_tree_params* p) {
 	for (int k = (int) levels.size() - 2; k >= 0; k--) {
 		const int64_t a = levels[k], e = levels[k + 1];
 		if (e > a) {
+			c->launches++;
 			k_upsweep<Ops><<<(int) std::min<int64_t>(e - a, (int64_t) c->nsm * 32), UTPB, 0, st>>>(a, e, b->nodes, b->nbox, b->multi, b->tbox, b->gbox,
 					b->x[0], b->x[1], b->x[2], p->bucket);
 		}

@@ -111,6 +111,8 @@ ct_status ct_ctx_create(ct_ctx** out, int device, size_t hbm_budget_bytes, int o
 void ct_ctx_destroy(ct_ctx* ctx);
 const char* ct_last_error(const ct_ctx* ctx);
 int ct_order(const ct_ctx* ctx);
+/* Number of this library's kernels launched on the context so far. */
+unsigned long long ct_launch_count(const ct_ctx* ctx);
 
 /* ---- boxes (independent periodic unit boxes with their own particles and tree) */
 ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id);
@@ -151,6 +153,13 @@ ct_status ct_synchronize(ct_ctx* ctx);
  * image plus the periodic correction, alpha = 2.  Results in double, unscaled by GM. */
 ct_status ct_direct_ewald(ct_ctx* ctx, int box_id, int64_t nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, double h, double* gx,
 		double* gy, double* gz, double* pot);
+
+/* Measured FP32 FMA throughput of the context's device in TFLOP/s (2 flops per FMA): the
+ * denominator of the FP32 roofline of the interaction kernels. */
+ct_status ct_fp32_peak(ct_ctx* ctx, double* tflops);
+
+/* The context's CUDA stream (cudaStream_t), for callers that order their own work with it. */
+void* ct_stream(ct_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -740,7 +740,9 @@ void walk(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const uint3
 				const float h3inv = h2inv * hinv;
 				for (int k = 0; k < nsinks; k++) {
 					const int s = self.part_begin + k;
-					float fx = 0.f, fy = 0.f, fz = 0.f, pot = 0.f;
+					// pairwise terms in FP32 as the reference computes them; sums kept in FP64 so that
+					// the oracle carries no accumulation error of its own
+					double fx = 0.0, fy = 0.0, fz = 0.0, pot = 0.0;
 					for (int c : leaflist) {
 						const ct_or_node& o = nodes[c];
 						for (int j = o.part_begin; j < o.part_end; j++) {
@@ -755,17 +757,17 @@ void walk(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const uint3
 							} else {
 								gsoft(r3inv, r1inv, r2, hinv, h2inv, h3inv);
 							}
-							fx = std::fma(dx0, r3inv, fx);
-							fy = std::fma(dx1, r3inv, fy);
-							fz = std::fma(dx2, r3inv, fz);
-							pot -= r1inv;
+							fx += double(dx0 * r3inv);
+							fy += double(dx1 * r3inv);
+							fz += double(dx2 * r3inv);
+							pot -= double(r1inv);
 						}
 						acc.flops += 21.0 * (o.part_end - o.part_begin);
 					}
-					force[k].gx -= fx;
-					force[k].gy -= fy;
-					force[k].gz -= fz;
-					force[k].phi += pot;
+					force[k].gx = float(double(force[k].gx) - fx);
+					force[k].gy = float(double(force[k].gy) - fy);
+					force[k].gz = float(double(force[k].gz) - fz);
+					force[k].phi = float(double(force[k].phi) + pot);
 				}
 			}
 		} else {
@@ -917,7 +919,8 @@ void collect(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const ui
 
 template<class Ops>
 int kick_impl(const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y, const uint32_t* z, float* v,
-		int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops) {
+		int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops, int stride = 1,
+		int64_t* sampled = nullptr) {
 	if (nnodes <= 0) {
 		return -1;
 	}
@@ -945,8 +948,19 @@ int kick_impl(const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, c
 	KickAcc top;
 	std::vector<WorkItem<Ops>> items;
 	collect<Ops>(C, top, root, L0, pos0, checks, checks, max_parts, items);
+	// a sampled run processes every stride-th work item (bounded CPU baseline)
+	std::vector<int> todo;
+	int64_t nsamp = 0;
+	for (int i = 0; i < (int) items.size(); i += std::max(stride, 1)) {
+		todo.push_back(i);
+		nsamp += nodes[items[i].self].part_end - nodes[items[i].self].part_begin;
+	}
+	if (sampled) {
+		*sampled = nsamp;
+	}
 	std::vector<KickAcc> accs(items.size());
-	parallel_for((int) items.size(), nthreads, [&](int i) {
+	parallel_for((int) todo.size(), nthreads, [&](int k) {
+		const int i = todo[k];
 		walk<Ops>(C, accs[i], items[i].self, items[i].L.data(), items[i].pos, items[i].e, items[i].d);
 	});
 	KickAcc tot = top;
@@ -1110,6 +1124,18 @@ int ct_or_kick(int order, const ct_or_kick_params* p, int nnodes, const ct_or_no
 		return kick_impl<Ops5>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops);
 	}
 	return kick_impl<Ops7>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops);
+}
+
+int ct_or_kick_sampled(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y,
+		const uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops,
+		int stride, int64_t* sampled) {
+	if (p->save_force && (!gx || !gy || !gz || !pot)) {
+		return -2;
+	}
+	if (order == 5) {
+		return kick_impl<Ops5>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops, stride, sampled);
+	}
+	return kick_impl<Ops7>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops, stride, sampled);
 }
 
 void ct_or_drift(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt, double drag) {

@@ -79,6 +79,12 @@ int ct_or_tree_build(int order, int n, int begin, uint32_t* x, uint32_t* y, uint
 int ct_or_kick(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y, const uint32_t* z,
 		float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops);
 
+/* Same kick on every stride-th top-level work item only (a bounded sample for CPU timing);
+ * *sampled receives the number of particles kicked. */
+int ct_or_kick_sampled(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y,
+		const uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops,
+		int stride, int64_t* sampled);
+
 /* Drift of one rung (src/drift.cu:36-154, lightcone excluded). */
 void ct_or_drift(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt, double drag);
 

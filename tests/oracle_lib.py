@@ -125,6 +125,24 @@ class Oracle:
             raise RuntimeError("oracle kick error %d" % err)
         return (gx, gy, gz, pot), rc, flops.value
 
+    def kick_sampled(self, params, nodes, x, y, z, v, rung, stride, order=7, nthreads=0):
+        """Kick of every stride-th top-level work item; returns (seconds, particles kicked, flops)."""
+        import time
+
+        n = len(x)
+        g = [np.zeros(n, np.float32) for _ in range(4)]
+        rc = KickReturn()
+        flops = ctypes.c_double(0)
+        sampled = ctypes.c_int64(0)
+        t = time.perf_counter()
+        err = self.lib.ct_or_kick_sampled(ctypes.c_int(order), ctypes.byref(params), ctypes.c_int(len(nodes)), _p(nodes), _p(x), _p(y), _p(z), _p(v),
+                                          _p(rung), *[_p(a) for a in g], ctypes.byref(rc), ctypes.c_int(nthreads), ctypes.byref(flops),
+                                          ctypes.c_int(stride), ctypes.byref(sampled))
+        dt = time.perf_counter() - t
+        if err:
+            raise RuntimeError("oracle kick error %d" % err)
+        return dt, sampled.value, flops.value
+
     def drift(self, x, y, z, v, rung, which_rung, a, dt, drag=0.0):
         self.lib.ct_or_drift(ctypes.c_int(len(x)), _p(x), _p(y), _p(z), _p(v), _p(rung), ctypes.c_int(which_rung), ctypes.c_float(a),
                              ctypes.c_float(dt), ctypes.c_double(drag))
