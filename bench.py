@@ -208,7 +208,6 @@ def main():
         ox, oy, oz = (torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32) for _ in range(3))
         ov = torch.empty((N, 3), dtype=torch.float32).pin_memory().numpy()
         orr = torch.empty(N, dtype=torch.int8).pin_memory().numpy()
-        import ctypes
 
         def e2e_step(first):
             box.upload(hx, hy, hz, hv, hr)
@@ -236,8 +235,6 @@ def main():
         e2e = {"value": N * world * ke / (ms_e / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(N * (12 + 12 + 1)),
                "d2h_bytes_per_step": int(N * (12 + 12 + 1))}
     # ---- roofline of the leaf kernel (reference flop convention)
-    import ctypes
-
     L = ctx.lib
     L.ct_fp32_peak.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
     pk = ctypes.c_double(0)

@@ -20,6 +20,7 @@
 //                centre, compensated per-batch accumulation), L2P and the kick
 //                (gravity.cu:157-211,246-404, kick.cu:53-177).
 #include <cub/cub.cuh>
+#include <cstdlib>
 
 #include "ct_internal.cuh"
 #include "ct_ops.cuh"
@@ -824,6 +825,286 @@ __global__ void __launch_bounds__(LEAF_TPB) k_leaf(LeafArgs a) {
 	}
 }
 
+// ---------------------------------------------------------------- split leaf path
+// P2P alone (warp per 32-sink tile of a leaf, sources staged per warp in shared memory as
+// float4 positions relative to the leaf centre), then M2P + L2P + kick per tile.
+constexpr int P2P_TPB = 256;
+constexpr int P2P_STAGE = 64;
+
+struct P2PArgs {
+	const NodeW* nodes;
+	const int2* items;  // (leaf node, tile)
+	int64_t nitems;
+	const int2* pp;
+	const int* pp_list;
+	const uint32_t* x[3];
+	float4* F;          // per particle: P2P sums (sum dx r^-3, ..., -sum r^-1)
+	float h;
+	int compensated;
+	double* pairs;
+};
+
+__global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
+	__shared__ float4 stage[P2P_TPB / 32][P2P_STAGE];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nw = (gridDim.x * blockDim.x) >> 5;
+	float4* my = stage[w];
+	const float h = a.h, h2 = h * h, hinv = 1.f / h, h2inv = hinv * hinv, h3inv = h2inv * hinv;
+	double npairs = 0.0;
+	for (int64_t it = gw; it < a.nitems; it += nw) {
+		const int2 item = a.items[it];
+		const NodeW self = a.nodes[item.x];
+		const int k = self.pbeg + 32 * item.y + lane;
+		const bool active = k < self.pend;
+		float kx = 0.f, ky = 0.f, kz = 0.f;
+		if (active) {
+			kx = fixed_dist(a.x[0][k], self.x);
+			ky = fixed_dist(a.x[1][k], self.y);
+			kz = fixed_dist(a.x[2][k], self.z);
+		}
+		float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, cp = 0.f;
+		const int2 ppl = a.pp[item.x];
+		int64_t np = 0;
+		for (int q = 0; q < ppl.y; q++) {
+			const NodeW src = a.nodes[a.pp_list[ppl.x + q]];
+			for (int c0 = src.pbeg; c0 < src.pend; c0 += P2P_STAGE) {
+				const int cnt = min(P2P_STAGE, src.pend - c0);
+				for (int j = lane; j < cnt; j += 32) {
+					const int pi = c0 + j;
+					my[j] = make_float4(fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z), 0.f);
+				}
+				__syncwarp();
+				float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
+#pragma unroll 4
+				for (int j = 0; j < cnt; j++) {
+					const float4 s = my[j];
+					const float dx = kx - s.x, dy = ky - s.y, dz = kz - s.z;
+					const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+					float r1inv, r3inv;
+					if (r2 > h2) {
+						r1inv = rsqrtf(r2);
+						r3inv = r1inv * r1inv * r1inv;
+					} else {
+						// Ferrer softening kernel (gravity.hpp:73-96)
+						const float q2 = r2 * h2inv;
+						float f = 315.f / 128.f;
+						f = fmaf(f, q2, -385.f / 32.f);
+						f = fmaf(f, q2, 1485.f / 64.f);
+						f = fmaf(f, q2, -693.f / 32.f);
+						f = fmaf(f, q2, 1155.f / 128.f);
+						r3inv = f * h3inv;
+						float ph = -63.f / 256.f;
+						ph = fmaf(ph, q2, 385.f / 256.f);
+						ph = fmaf(ph, q2, -495.f / 128.f);
+						ph = fmaf(ph, q2, 693.f / 128.f);
+						ph = fmaf(ph, q2, -1155.f / 256.f);
+						ph = fmaf(ph, q2, 693.f / 256.f);
+						r1inv = ph * hinv;
+					}
+					fx = fmaf(dx, r3inv, fx);
+					fy = fmaf(dy, r3inv, fy);
+					fz = fmaf(dz, r3inv, fz);
+					pt -= r1inv;
+				}
+				__syncwarp();
+				if (a.compensated) {
+					ksum(sx, cx, fx);
+					ksum(sy, cy, fy);
+					ksum(sz, cz, fz);
+					ksum(sp, cp, pt);
+				} else {
+					sx += fx;
+					sy += fy;
+					sz += fz;
+					sp += pt;
+				}
+				np += cnt;
+			}
+		}
+		if (active) {
+			a.F[k] = make_float4(sx + cx, sy + cy, sz + cz, sp + cp);
+			npairs += (double) np;
+		}
+	}
+	for (int o = 16; o; o >>= 1) {
+		npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
+	}
+	if (lane == 0 && npairs > 0) {
+		atomicAdd(a.pairs, npairs);
+	}
+}
+
+struct KickTileArgs {
+	const NodeW* nodes;
+	const float* multi;
+	const float* Lx;
+	const int2* items;
+	int64_t nitems;
+	const int2* pc;
+	const int* pc_list;
+	const float4* F;
+	const uint32_t* x[3];
+	float* v[3];
+	int8_t* rung;
+	float* g[3];
+	float* pot;
+	ct_kick_params kp;
+	double* sums;
+	int* max_rung;
+};
+
+// M2P, L2P and the kick for one 32-sink tile per warp (gravity.cu:157-211, kick.cu:53-177).
+template<class Ops>
+__global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
+	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
+	__shared__ double s_red[4][9];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nw = (gridDim.x * blockDim.x) >> 5;
+	const auto& kp = a.kp;
+	const float hinv = 1.f / kp.h;
+	double acc[9];
+	for (int q = 0; q < 9; q++) {
+		acc[q] = 0.0;
+	}
+	int maxr = 0;
+	for (int64_t it = gw; it < a.nitems; it += nw) {
+		const int2 item = a.items[it];
+		const NodeW self = a.nodes[item.x];
+		const int k = self.pbeg + 32 * item.y + lane;
+		const bool active = k < self.pend;
+		uint32_t X[3] = { self.x, self.y, self.z };
+		if (active) {
+			X[0] = a.x[0][k];
+			X[1] = a.x[1][k];
+			X[2] = a.x[2][k];
+		}
+		float Fx = 0.f, Fy = 0.f, Fz = 0.f, Fp = (693.f / 256.f) * hinv;
+		const int2 pcl = a.pc[item.x];
+		for (int q = 0; q < pcl.y; q++) {
+			const int c = a.pc_list[pcl.x + q];
+			const NodeW ot = a.nodes[c];
+			float M[NM], D[NE], L2[5] = { 0.f, 0.f, 0.f, 0.f, 0.f };
+			const float* mp = a.multi + (size_t) NMULT_STRIDE * c;
+			for (int i = 0; i < NM; i++) {
+				M[i] = __ldg(mp + i);
+			}
+			Ops::greens(D, fixed_dist(X[0], ot.x), fixed_dist(X[1], ot.y), fixed_dist(X[2], ot.z));
+			Ops::m2l2(L2, M, D, kp.do_phi != 0);
+			Fx -= 1e6f * L2[1];
+			Fy -= 1e6f * L2[2];
+			Fz -= 1e6f * L2[3];
+			Fp += 1e3f * L2[0];
+		}
+		if (!active) {
+			continue;
+		}
+		acc[8] += pcl.y;
+		const float4 P = a.F[k];
+		Fx -= P.x;
+		Fy -= P.y;
+		Fz -= P.z;
+		Fp += P.w;
+		float La[NE], L2[5];
+		const float* Lsrc = a.Lx + (size_t) NEXP_STRIDE * item.x;
+		for (int i = 0; i < NE; i++) {
+			La[i] = Lsrc[i];
+		}
+		Ops::l2p(L2, La, fixed_dist(X[0], self.x), fixed_dist(X[1], self.y), fixed_dist(X[2], self.z), kp.do_phi != 0);
+		Fp += 1e3f * L2[0];
+		Fx -= 1e6f * L2[1];
+		Fy -= 1e6f * L2[2];
+		Fz -= 1e6f * L2[3];
+		Fz *= kp.GM;
+		Fy *= kp.GM;
+		Fx *= kp.GM;
+		Fp *= kp.GM;
+		float vx = a.v[0][k], vy = a.v[1][k], vz = a.v[2][k];
+		const float kin0 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
+		const float sgn = kp.sign * (kp.top ? 1.f : -1.f);
+		const float rdt = 1.0f / (float) (1 << kp.min_rung);
+		if (kp.ascending) {
+			const float dt = 0.5f * rdt * kp.t0;
+			if (!kp.first_call) {
+				vx = fmaf(sgn * Fx, dt, vx);
+				vy = fmaf(sgn * Fy, dt, vy);
+				vz = fmaf(sgn * Fz, dt, vz);
+			}
+		}
+		acc[1] += 0.5f * (vx * vx + vy * vy + vz * vz);
+		acc[3] += vx;
+		acc[4] += vy;
+		acc[5] += vz;
+		acc[6] += sqrtf(vx * vx + vy * vy + vz * vz);
+		if (kp.save_force) {
+			a.g[0][k] = Fx;
+			a.g[1][k] = Fy;
+			a.g[2][k] = Fz;
+			a.pot[k] = Fp;
+		}
+		if (kp.descending) {
+			const float g2 = Fx * Fx + Fy * Fy + Fz * Fz;
+			float dt = fminf(kp.eta * sqrtf(kp.a * kp.h * rsqrtf(g2)), kp.t0);
+			dt = fminf(kp.max_dt, dt);
+			int r = a.rung[k];
+			r = max(kp.min_rung + int((int) ceilf(log2f(kp.t0 / dt)) > kp.min_rung), r - 1);
+			r = max(0, min(r, 15));
+			a.rung[k] = (int8_t) r;
+			maxr = max(maxr, r);
+			dt = 0.5f * rdt * kp.t0;
+			vx = fmaf(sgn * Fx, dt, vx);
+			vy = fmaf(sgn * Fy, dt, vy);
+			vz = fmaf(sgn * Fz, dt, vz);
+		}
+		const float kin1 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
+		a.v[0][k] = vx;
+		a.v[1][k] = vy;
+		a.v[2][k] = vz;
+		acc[0] += 0.5f * Fp;
+		acc[2] += kin1 - kin0;
+	}
+	for (int q = 0; q < 9; q++) {
+		double v = acc[q];
+		for (int o = 16; o; o >>= 1) {
+			v += __shfl_xor_sync(0xffffffffu, v, o);
+		}
+		if (lane == 0) {
+			s_red[w][q] = v;
+		}
+	}
+	for (int o = 16; o; o >>= 1) {
+		maxr = max(maxr, __shfl_xor_sync(0xffffffffu, maxr, o));
+	}
+	__syncthreads();
+	if (threadIdx.x < 9) {
+		double v = 0;
+		for (int q = 0; q < 4; q++) {
+			v += s_red[q][threadIdx.x];
+		}
+		atomicAdd(a.sums + threadIdx.x, v);
+	}
+	if (lane == 0 && maxr > 0) {
+		atomicMax(a.max_rung, maxr);
+	}
+}
+
+// 32-sink tiles of every leaf: counts, then (leaf, tile) items at the scanned offsets.
+__global__ void k_tile_count(int64_t nleaves, const int64_t* leaves, const NodeW* nodes, int* ntiles) {
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nleaves; i += (int64_t) gridDim.x * blockDim.x) {
+		const NodeW nd = nodes[leaves[i]];
+		ntiles[i] = (nd.pend - nd.pbeg + 31) / 32;
+	}
+}
+__global__ void k_tile_fill(int64_t nleaves, const int64_t* leaves, const int* ntiles, const int* off, int2* items) {
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nleaves; i += (int64_t) gridDim.x * blockDim.x) {
+		const int o = off[i];
+		for (int t = 0; t < ntiles[i]; t++) {
+			items[o + t] = make_int2((int) leaves[i], t);
+		}
+	}
+}
+
 __global__ void k_collect_leaves(int64_t nn, const NodeW* nodes, int64_t* leaves, unsigned long long* count) {
 	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nn; i += (int64_t) gridDim.x * blockDim.x) {
 		const NodeW nd = nodes[i];
@@ -1010,12 +1291,76 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		la.compensated = 1;
 		la.sums = counters + 4;
 		la.max_rung = c->d_flags + 48;
-		cudaEventRecord(c->ev[4], st);
-		if (nleaves > 0) {
+		static const bool fused = getenv("CT_LEAF_FUSED") != nullptr;
+		if (fused) {
+			cudaEventRecord(c->ev[4], st);
+			if (nleaves > 0) {
+				c->launches++;
+				k_leaf<Ops><<<(int) std::min<int64_t>(nleaves, (int64_t) c->nsm * 16), LEAF_TPB, 0, st>>>(la);
+			}
+			cudaEventRecord(c->ev[5], st);
+		} else if (nleaves > 0) {
+			// 32-sink tiles of the leaves
+			ct_status s2 = CT_OK;
+			int* ntl = (int*) scratch(c, 40, sizeof(int) * (nleaves + 1), &s2);
+			int* off = (int*) scratch(c, 41, sizeof(int) * (nleaves + 1), &s2);
+			CT_TRY(s2);
+			size_t need = 0;
+			cub::DeviceScan::ExclusiveSum(nullptr, need, ntl, off, (int) nleaves + 1, st);
+			void* tmp = scratch(c, 42, need + 256, &s2);
+			CT_TRY(s2);
 			c->launches++;
-			k_leaf<Ops><<<(int) std::min<int64_t>(nleaves, (int64_t) c->nsm * 16), LEAF_TPB, 0, st>>>(la);
+			k_tile_count<<<(int) std::max<int64_t>(1, std::min<int64_t>((nleaves + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nleaves, K.leaves, b->nodes, ntl);
+			CT_CUDA(c, cudaMemsetAsync(ntl + nleaves, 0, sizeof(int), st));
+			CT_CUDA(c, cub::DeviceScan::ExclusiveSum(tmp, need, ntl, off, (int) nleaves + 1, st));
+			CT_CUDA(c, cudaMemcpyAsync(hf, off + nleaves, sizeof(int), cudaMemcpyDeviceToHost, st));
+			CT_CUDA(c, cudaStreamSynchronize(st));
+			const int64_t nitems = hf[0];
+			int2* items = (int2*) scratch(c, 43, sizeof(int2) * (nitems + 1), &s2);
+			float4* F = (float4*) scratch(c, 44, sizeof(float4) * b->n, &s2);
+			CT_TRY(s2);
+			c->launches++;
+			k_tile_fill<<<(int) std::max<int64_t>(1, std::min<int64_t>((nleaves + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nleaves, K.leaves, ntl, off, items);
+			P2PArgs pa;
+			pa.nodes = b->nodes;
+			pa.items = items;
+			pa.nitems = nitems;
+			pa.pp = o.pp;
+			pa.pp_list = o.pp_list;
+			for (int d = 0; d < 3; d++) {
+				pa.x[d] = b->x[d];
+			}
+			pa.F = F;
+			pa.h = kp->h;
+			pa.compensated = 1;
+			pa.pairs = counters + 4 + 7;
+			cudaEventRecord(c->ev[4], st);
+			c->launches++;
+			k_p2p<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
+			cudaEventRecord(c->ev[5], st);
+			KickTileArgs ka;
+			ka.nodes = b->nodes;
+			ka.multi = b->multi;
+			ka.Lx = K.Lx;
+			ka.items = items;
+			ka.nitems = nitems;
+			ka.pc = o.pc;
+			ka.pc_list = o.pc_list;
+			ka.F = F;
+			for (int d = 0; d < 3; d++) {
+				ka.x[d] = b->x[d];
+				ka.v[d] = b->v[d];
+				ka.g[d] = b->g[d];
+			}
+			ka.rung = b->rung;
+			ka.pot = b->pot;
+			ka.kp = *kp;
+			ka.sums = counters + 4;
+			ka.max_rung = c->d_flags + 48;
+			c->launches++;
+			k_leaf_kick<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 3) / 4, (int64_t) c->nsm * 16)), 128, 0, st>>>(ka);
+			cudaEventRecord(c->ev[12], st);
 		}
-		cudaEventRecord(c->ev[5], st);
 		CT_CUDA(c, cudaGetLastError());
 		double* hd = (double*) c->pinned;
 		CT_CUDA(c, cudaMemcpyAsync(hd, counters, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1060,7 +1405,11 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
 		C.ms_l2l = ms;
 		cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
-		C.ms_leaf = ms;
+		C.ms_leaf = ms;  // the P2P kernel (or the fused leaf kernel)
+		if (!fused && nleaves > 0) {
+			cudaEventElapsedTime(&ms, c->ev[5], c->ev[12]);
+			C.ms_leafkick = ms;
+		}
 		b->have_force = kp->save_force != 0;
 		return CT_OK;
 	}

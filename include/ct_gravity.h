@@ -104,6 +104,7 @@ typedef struct {
 	double flops_pp;
 	double flops_cc;
 	double ms_tree, ms_walk, ms_m2l, ms_l2l, ms_leaf, ms_drift; /* device time of the last calls */
+	double ms_leafkick;   /* M2P + L2P + kick after the P2P kernel */
 } ct_counters;
 
 /* ---- context */

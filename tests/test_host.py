@@ -1,0 +1,111 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports every declared
+entry point, the package fails loudly without a device, box sharding and the multi-rank
+aggregation (gloo, world size 2), and the initial-condition generators."""
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "ct_gravity.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ct_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    from cosmictiger_b200 import LIB_PATH, build
+
+    if not os.path.exists(LIB_PATH):
+        build.build()
+    out = subprocess.check_output(["nm", "-D", "--defined-only", LIB_PATH], text=True)
+    exported = set(ln.split()[-1] for ln in out.splitlines() if ln.strip())
+    want = declared_symbols()
+    assert len(want) >= 15
+    missing = [s for s in want if s not in exported]
+    assert not missing, missing
+
+
+def test_library_loads_and_context_needs_a_device():
+    import cosmictiger_b200 as ct
+
+    ct.library()
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(ct.GravityError):
+        ct.Context(device=0)
+
+
+def test_shard_boxes_partition():
+    from cosmictiger_b200.ensemble import shard_boxes
+
+    rng = np.random.default_rng(0)
+    sizes = (np.exp(rng.uniform(np.log(16), np.log(128), 512)).astype(int)) ** 3
+    for world in (1, 2, 3, 8):
+        parts = [shard_boxes(sizes, world, r) for r in range(world)]
+        allidx = np.sort(np.concatenate(parts))
+        assert np.array_equal(allidx, np.arange(len(sizes)))
+        loads = [sizes[p].sum() for p in parts]
+        assert max(loads) - min(loads) <= sizes.max()
+
+
+_GLOO = r'''
+import os, sys
+sys.path.insert(0, %r)
+import torch.distributed as dist
+from cosmictiger_b200.ensemble import aggregate, shard_boxes
+dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d", rank=int(sys.argv[1]), world_size=2)
+r = dist.get_rank()
+mine = shard_boxes([10, 20, 30, 40, 50], 2, r)
+ms = 100.0 + 50.0 * r
+val, tmax = aggregate(ms, 1000.0 * (r + 1), dist)
+print("RESULT", r, list(mine), val, tmax, flush=True)
+dist.barrier()
+dist.destroy_process_group()
+'''
+
+
+def test_two_rank_aggregation_gloo(tmp_path):
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    script = tmp_path / "agg.py"
+    script.write_text(_GLOO % (ROOT, port))
+    procs = [subprocess.Popen([sys.executable, str(script), str(r)], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True) for r in range(2)]
+    outs = [p.communicate(timeout=120)[0] for p in procs]
+    assert all(p.returncode == 0 for p in procs), outs
+    res = {}
+    for o in outs:
+        for ln in o.splitlines():
+            if ln.startswith("RESULT"):
+                f = ln.split(maxsplit=3)
+                res[int(f[1])] = f
+    assert set(res) == {0, 1}
+    # sum of particle-steps 3000 over the max time 150 ms
+    for r in (0, 1):
+        tail = res[r][3].rsplit(" ", 2)
+        assert abs(float(tail[1]) - 3000.0 / 0.15) < 1e-6
+        assert abs(float(tail[2]) - 150.0) < 1e-9
+
+
+def test_ics_fixed_point_and_shapes():
+    from cosmictiger_b200 import ics
+
+    x, y, z, v, r = ics.zeldovich_lattice(8, index=-2.0, rms_spacing=0.25, seed=1)
+    assert x.dtype == np.uint32 and v.shape == (512, 3) and r.dtype == np.int8
+    disp = ics.fixed32_to_double(x) - np.repeat(np.arange(8) / 8.0, 64)
+    disp = (disp + 0.5) % 1.0 - 0.5
+    assert 0.0 < np.sqrt(np.mean(disp ** 2)) < 0.25 / 8
+    cx, cy, cz, cv, cr = ics.clustered_box(16, nspheres=20, seed=2)
+    assert len(cx) == 16 ** 3
+    assert ics.to_fixed32(np.array([0.0, 0.5, 1.0 - 1e-12, -0.25]))[1] == 2 ** 31
