@@ -19,7 +19,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
 UNITS = {
     "ct_tree.cu": ["-fmad=false"],
-    "ct_kick.cu": [],
+    "ct_kick.cu": ["-fmad=false"],
     "ct_api.cu": [],
 }
 

@@ -97,13 +97,75 @@ CT_HD_FN T ct_erf_series(T x) {
 	return w * x;
 }
 
+// Single-precision exp and sincos used inside the Ewald operator.  They are written here (not
+// taken from the CUDA or C math library) so that host and device evaluate them with the same
+// IEEE operation sequence and agree bit for bit:
+//   exp:    Cody-Waite reduction y = k ln2 + r (ln2 split in two parts, |r| <= ln2/2), Taylor
+//           polynomial of exp(r) through r^8 (truncation < 2e-9), exact scaling by 2^k;
+//   sincos: Cody-Waite reduction by pi/2 (three-part split), Taylor polynomials of sin through
+//           r^11 and cos through r^12 on |r| <= pi/4, quadrant selection.
+CT_HD_FN float ct_exp_poly(float y) {
+	if (y < -87.0f) {
+		return 0.0f;
+	}
+	const float k = rintf(y * 1.44269504088896341f);
+	float r = ct_fma(-k, 0.693145751953125f, y);
+	r = ct_fma(-k, 1.428606765330187e-06f, r);
+	float p = 1.0f / 40320.0f;
+	p = ct_fma(p, r, 1.0f / 5040.0f);
+	p = ct_fma(p, r, 1.0f / 720.0f);
+	p = ct_fma(p, r, 1.0f / 120.0f);
+	p = ct_fma(p, r, 1.0f / 24.0f);
+	p = ct_fma(p, r, 1.0f / 6.0f);
+	p = ct_fma(p, r, 0.5f);
+	p = ct_fma(p, r, 1.0f);
+	p = ct_fma(p, r, 1.0f);
+	return ldexpf(p, (int) k);
+}
+CT_HD_FN void ct_sincos_poly(float x, float* s, float* c) {
+	const float k = rintf(x * 0.636619772367581343f);
+	float r = ct_fma(-k, 1.5707963705062866f, x);
+	r = ct_fma(-k, -4.371138828673793e-08f, r);
+	r = ct_fma(-k, -1.7763568394002505e-15f, r);
+	const float r2 = r * r;
+	float ps = -1.0f / 39916800.0f;
+	ps = ct_fma(ps, r2, 1.0f / 362880.0f);
+	ps = ct_fma(ps, r2, -1.0f / 5040.0f);
+	ps = ct_fma(ps, r2, 1.0f / 120.0f);
+	ps = ct_fma(ps, r2, -1.0f / 6.0f);
+	const float sr = ct_fma(ps * r2, r, r);
+	float pc = 1.0f / 479001600.0f;
+	pc = ct_fma(pc, r2, -1.0f / 3628800.0f);
+	pc = ct_fma(pc, r2, 1.0f / 40320.0f);
+	pc = ct_fma(pc, r2, -1.0f / 720.0f);
+	pc = ct_fma(pc, r2, 1.0f / 24.0f);
+	pc = ct_fma(pc, r2, -0.5f);
+	const float cr = ct_fma(pc, r2, 1.0f);
+	const int q = ((int) k) & 3;
+	const float S[4] = { sr, cr, -sr, -cr };
+	const float C[4] = { cr, -sr, -cr, sr };
+	*s = S[q];
+	*c = C[q];
+}
+CT_HD_FN double ct_exp_poly(double y) {
+	return exp(y);
+}
+CT_HD_FN void ct_sincos_poly(double x, double* s, double* c) {
+#ifdef __CUDA_ARCH__
+	sincos(x, s, c);
+#else
+	*s = std::sin(x);
+	*c = std::cos(x);
+#endif
+}
+
 // erfc(x) and exp(-x^2) by Abramowitz & Stegun 7.1.26 (|error| <= 1.5e-7), the form the
 // reference uses on the device (cosmictiger/math.hpp:56-71).
 template<class T>
 CT_HD_FN void ct_erfcexp(T x, T* ec, T* ex) {
 	const T p = T(0.3275911), a1 = T(0.254829592), a2 = T(-0.284496736), a3 = T(1.421413741), a4 = T(-1.453152027), a5 = T(1.061405429);
 	const T t = T(1) / ct_fma(p, x, T(1));
-	*ex = ct_exp_f(-x * x);
+	*ex = ct_exp_poly(-x * x);
 	T s = ct_fma(a5, t, a4);
 	s = ct_fma(s, t, a3);
 	s = ct_fma(s, t, a2);

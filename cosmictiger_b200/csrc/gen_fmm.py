@@ -191,13 +191,18 @@ def emit_sum(em, target, terms, init, op="="):
         if c == 0:
             continue
         groups.setdefault(c, []).append(e)
-    first = init
     parts = []
     for c in sorted(groups, key=lambda c: (abs(c), c)):
         exprs = groups[c]
-        acc = exprs[0]
+        # products are chained through explicit fused multiply-adds, so that host and device
+        # builds evaluate the same operation sequence (no compiler contraction choices)
+        e0 = exprs[0]
+        acc = "(%s * %s)" % e0 if isinstance(e0, tuple) else e0
         for e in exprs[1:]:
-            acc = "(%s + %s)" % (acc, e)
+            if isinstance(e, tuple):
+                acc = "ct_fma(%s, %s, %s)" % (e[0], e[1], acc)
+            else:
+                acc = "(%s + %s)" % (acc, e)
         parts.append((c, acc))
     if not parts:
         em("%s = %s;" % (target, init if init else "T(0)"))
@@ -296,7 +301,7 @@ def gen_radial(P):
         for m in half_range(n):
             m0 = sum(m)
             c = Fr(vfact(n), (2 ** m0) * vfact(m) * vfact(sub(n, add(m, m))))
-            terms.append((c, "(%s * G%d_%d)" % (mon[sub(n, add(m, m))], N - m0, m0)))
+            terms.append((c, (mon[sub(n, add(m, m))], "G%d_%d" % (N - m0, m0))))
         emit_sum(em, "Dr[%d]" % sym_index(n), terms, "Dr[%d]" % sym_index(n))
     return em.text()
 
@@ -348,7 +353,7 @@ def gen_m2l(P, Pmax):
     Mf = full_from_stored(em, "M", "Mf", P - 1, needM)
     Df = full_from_stored(em, "D", "Df", P, needD)
     for n in outs:
-        terms = [(Fr(1, vfact(m)), "(%s * %s)" % (Mf[m], Df[add(n, m)])) for m in plan[n]]
+        terms = [(Fr(1, vfact(m)), (Mf[m], Df[add(n, m)])) for m in plan[n]]
         idx = tl_index(n, Pmax)
         if n == (0, 0, 0):
             em("if (do_phi) {")
@@ -393,7 +398,7 @@ def gen_p2m(P):
             c = detrace_coef(n, m) / dfact(2 * N - 1)
             e = mon[sub(n, add(m, m))]
             if m0 > 0:
-                e = "(%s * q%d)" % (e, m0)
+                e = (e, "q%d" % m0)
             terms.append((c, e))
         emit_sum(em, "M[%d]" % idx, terms, None)
     return em.text()
@@ -415,7 +420,7 @@ def gen_m2m(P):
                     k = (a, b, c)
                     coef = Fr(vfact(n), vfact(k) * vfact(sub(n, k)))
                     d = sub(n, k)
-                    e = Mf[k] if d == (0, 0, 0) else "(%s * %s)" % (mon[d], Mf[k])
+                    e = Mf[k] if d == (0, 0, 0) else (mon[d], Mf[k])
                     terms.append((coef, e))
         emit_sum(em, "Mb[%d]" % sym_index(n), terms, None)
     em.lines.extend(gen_detrace_full(Q, "Mb", "M").splitlines())
@@ -444,7 +449,7 @@ def gen_l2l(P, Qout):
     for n in outs:
         terms = []
         for k in plan[n]:
-            e = Lf[add(n, k)] if k == (0, 0, 0) else "(%s * %s)" % (mon[k], Lf[add(n, k)])
+            e = Lf[add(n, k)] if k == (0, 0, 0) else (mon[k], Lf[add(n, k)])
             terms.append((Fr(1, vfact(k)), e))
         idx = tl_index(n, Qout)
         if n == (0, 0, 0):
@@ -643,7 +648,7 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 	for (int i = 0; i < CT_EWALD_NFOUR; i++) {
 		const T hdotx = ct_fma(T(tab.four[i][0]), x, ct_fma(T(tab.four[i][1]), y, T(tab.four[i][2]) * z));
 		T sn, cn;
-		ct_sincos(T(6.2831853071795865e-3) * hdotx, &sn, &cn);
+		ct_sincos_poly(T(6.2831853071795865e-3) * hdotx, &sn, &cn);
 		for (int k = 0; k < NEXP; k++) {
 			const int order = CT_TAB(EXP_IDX)[k][0] + CT_TAB(EXP_IDX)[k][1] + CT_TAB(EXP_IDX)[k][2];
 			Df[k] = ct_fma((order & 1) ? sn : cn, T(tab.four_exp[i][k]), Df[k]);
