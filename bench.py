@@ -46,7 +46,96 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--accuracy-sinks", type=int, default=0, help="FP64 direct-Ewald check on this many sinks (0: skip)")
+    ap.add_argument("--ensemble-boxes", type=int, default=64, help="boxes of the batched-vs-plain ensemble comparison (0: skip)")
+    ap.add_argument("--ensemble-nmin", type=int, default=16)
+    ap.add_argument("--ensemble-nmax", type=int, default=64)
+    ap.add_argument("--ensemble-steps", type=int, default=3)
     return ap.parse_args()
+
+
+def make_ensemble(nbox, nmin, nmax, seed):
+    """nbox boxes of n_i^3 particles, n_i log-uniform in [nmin, nmax] (seeded), each with its
+    own Zel'dovich field: spectral index uniform in [-2.5, -1], RMS displacement uniform in
+    0.1-0.6 mean spacings."""
+    from cosmictiger_b200 import ics
+
+    rng = np.random.default_rng(seed)
+    ns = np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax), nbox))).astype(int)
+    idx = rng.uniform(-2.5, -1.0, nbox)
+    rms = rng.uniform(0.1, 0.6, nbox)
+    boxes = [ics.zeldovich_lattice(int(n), index=float(i), rms_spacing=float(r), seed=int(seed * 1000 + k)) for k, (n, i, r) in enumerate(zip(ns, idx, rms))]
+    return boxes
+
+
+def ensemble_compare(ct, torch, ctx, args, theta, lib_stream):
+    """Aggregate particle-steps/s of an ensemble run as one batched ensemble vs the plain
+    single-box path launched box by box; per-box latency percentiles of the plain path."""
+    from cosmictiger_b200 import ics
+
+    sets = make_ensemble(args.ensemble_boxes, args.ensemble_nmin, args.ensemble_nmax, seed=4)
+    counts = [len(s[0]) for s in sets]
+    N = int(np.sum(counts))
+    h = ics.softening(float(np.mean(counts)), 0.02)
+    eta = ics.eta_default()
+    t0 = 1.0 / 64
+    hs = np.array([ics.softening(n, 0.02) for n in counts], np.float32)
+    gms = np.array([1.0 / n for n in counts], np.float32)
+    ens = ctx.ensemble(counts)
+    ens.upload(*[np.concatenate([s[k] for s in sets]) for k in range(5)])
+    ens.set_box_params(hs, gms)
+
+    def ens_step(first):
+        ens.tree_create(theta, float(hs.max()), 128)
+        ens.kick(ct.KickParams.make(theta=theta, h=float(hs.max()), GM=1.0 / N, eta=eta, t0=t0, first_call=first, save_force=False))
+        ens.drift(0, 1.0, t0)
+
+    plain = []
+    for s in sets:
+        bx = ctx.box(len(s[0]))
+        bx.upload(*s)
+        plain.append(bx)
+
+    def plain_step(first, lat=None):
+        for k, bx in enumerate(plain):
+            t = time.perf_counter()
+            bx.tree_create(theta, float(hs.max()), 128)
+            bx.kick(ct.KickParams.make(theta=theta, h=float(hs[k]), GM=float(gms[k]), eta=eta, t0=t0, first_call=first, save_force=False))
+            bx.drift(0, 1.0, t0)
+            if lat is not None:
+                ctx.synchronize()
+                lat.append((time.perf_counter() - t) * 1e3)
+
+    for i in range(2):
+        ens_step(i == 0)
+        plain_step(i == 0)
+    ctx.synchronize()
+    K = args.ensemble_steps
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    for i in range(K):
+        ens_step(False)
+    e1.record(lib_stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    e0.record(lib_stream)
+    for i in range(K):
+        plain_step(False)
+    e1.record(lib_stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ms_p = e0.elapsed_time(e1)
+    lat = []
+    plain_step(False, lat)
+    for bx in plain:
+        bx.close()
+    ens.close()
+    vb = N * K / (ms_b / 1e3)
+    vp = N * K / (ms_p / 1e3)
+    return {"boxes": len(counts), "particles": N, "n_range": [args.ensemble_nmin, args.ensemble_nmax], "steps": K,
+            "batched_particle_steps_s": vb, "plain_particle_steps_s": vp, "speedup": vb / vp,
+            "batched_ms_per_step": ms_b / K, "plain_box_ms_p50": float(np.percentile(lat, 50)), "plain_box_ms_p99": float(np.percentile(lat, 99))}
 
 
 def make_ics(args, seed):
@@ -252,6 +341,9 @@ def main():
     extra = {"ms_tree": float(np.mean(tree_ms)), "ms_walk": float(np.mean(walk_ms)), "ms_m2l": float(np.mean(m2l_ms)), "ms_leaf": float(np.mean(leaf_ms)),
              "pp_pairs": c["pp_pairs"], "cc_direct": c["cc_direct"], "cc_ewald": c["cc_ewald"], "pc_pairs": c["pc_pairs"], "cp_pairs": c["cp_pairs"],
              "nodes": c["nodes"], "leaves": c["leaves"], "flops_per_step": c["flops"], "wall_s": wall}
+    ens_res = None
+    if args.ensemble_boxes > 0:
+        ens_res = ensemble_compare(ct, torch, ctx, args, theta, lib_stream)
     acc = None
     if args.accuracy_sinks and rank == 0:
         acc = accuracy(box, args.accuracy_sinks, h, N)
@@ -286,6 +378,8 @@ def main():
         }
         if acc:
             line["force_error"] = acc
+        if ens_res:
+            line["ensemble"] = ens_res
         print(json.dumps(line), flush=True)
     box.close()
     ctx.close()

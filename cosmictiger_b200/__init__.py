@@ -135,6 +135,10 @@ def library():
     L.ct_tree_download.argtypes = [vp, i32, vp, i64, ctypes.POINTER(i64)]
     L.ct_get_counters.argtypes = [vp, i32, ctypes.POINTER(Counters)]
     L.ct_synchronize.argtypes = [vp]
+    L.ct_ensemble_create.argtypes = [vp, i32, ctypes.POINTER(i64), ctypes.POINTER(i32)]
+    L.ct_box_count.argtypes = [vp, i32]
+    L.ct_ensemble_set_params.argtypes = [vp, i32, vp, vp]
+    L.ct_kick_ensemble.argtypes = [vp, i32, ctypes.POINTER(KickParams), ctypes.POINTER(KickReturn)]
     L.ct_launch_count.argtypes = [vp]
     L.ct_launch_count.restype = ctypes.c_ulonglong
     L.ct_direct_ewald.argtypes = [vp, i32, i64, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
@@ -165,6 +169,10 @@ class Context:
     def box(self, n):
         return Box(self, n)
 
+    def ensemble(self, counts):
+        """Independent periodic boxes handled together (ct_ensemble_create)."""
+        return Box(self, int(np.sum(counts)), counts=counts)
+
     def launches(self):
         """Kernels of libct_gravity launched on this context so far."""
         return int(self.lib.ct_launch_count(self.h))
@@ -187,13 +195,35 @@ class Context:
 class Box:
     """A periodic unit box of particles with its tree, resident on the device."""
 
-    def __init__(self, ctx, n):
+    def __init__(self, ctx, n, counts=None):
         self.ctx = ctx
         self.n = int(n)
         bid = ctypes.c_int()
-        ctx.check(ctx.lib.ct_box_create(ctx.h, self.n, ctypes.byref(bid)), "ct_box_create")
+        if counts is None:
+            ctx.check(ctx.lib.ct_box_create(ctx.h, self.n, ctypes.byref(bid)), "ct_box_create")
+            self.counts = np.array([self.n], np.int64)
+        else:
+            self.counts = np.ascontiguousarray(counts, np.int64)
+            ctx.check(ctx.lib.ct_ensemble_create(ctx.h, len(self.counts), self.counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(bid)),
+                      "ct_ensemble_create")
         self.id = bid.value
         self.tree_params = None
+
+    @property
+    def nbox(self):
+        return len(self.counts)
+
+    def set_box_params(self, h, GM):
+        """Per-box softening and GM of an ensemble."""
+        h = np.ascontiguousarray(h, np.float32)
+        GM = np.ascontiguousarray(GM, np.float32)
+        self.ctx.check(self.ctx.lib.ct_ensemble_set_params(self.ctx.h, self.id, _p(h), _p(GM)), "ct_ensemble_set_params")
+
+    def kick_ensemble(self, params):
+        """Per-box kick returns of an ensemble."""
+        out = (KickReturn * self.nbox)()
+        self.ctx.check(self.ctx.lib.ct_kick_ensemble(self.ctx.h, self.id, ctypes.byref(params), out), "ct_kick_ensemble")
+        return list(out)
 
     def upload(self, x, y, z, vxyz, rung):
         """Host arrays: x,y,z uint32 fixed32; vxyz float32 (n,3); rung int8."""

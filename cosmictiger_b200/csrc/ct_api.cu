@@ -563,10 +563,16 @@ int ct_order(const ct_ctx* ctx) {
 	return ctx ? ((const Ctx*) ctx)->order : 0;
 }
 
-ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id) {
-	Ctx* c = (Ctx*) ctx;
-	if (!c || n < 0 || !box_id || n > (int64_t) INT32_MAX / 2) {
-		return fail(c, CT_ERR_ARG, "ct_box_create: bad arguments");
+static ct_status box_create_impl(Ctx* c, int nsub, const int64_t* counts, int* box_id) {
+	int64_t n = 0;
+	for (int s = 0; s < nsub; s++) {
+		if (counts[s] < 0) {
+			return fail(c, CT_ERR_ARG, "negative particle count");
+		}
+		n += counts[s];
+	}
+	if (n > (int64_t) INT32_MAX / 2) {
+		return fail(c, CT_ERR_ARG, "too many particles for 32-bit indices");
 	}
 	cudaSetDevice(c->device);
 	Box* b = new (std::nothrow) Box();
@@ -574,8 +580,22 @@ ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id) {
 		return fail(c, CT_ERR_MEMORY, "host allocation");
 	}
 	b->n = n;
+	b->nsub = nsub;
+	b->sub_off.assign(nsub + 1, 0);
+	for (int s = 0; s < nsub; s++) {
+		b->sub_off[s + 1] = b->sub_off[s] + counts[s];
+	}
 	memset(&b->counters, 0, sizeof(b->counters));
-	ct_status s = CT_OK;
+	ct_status s = dalloc(c, (void**) &b->d_sub_off, sizeof(int64_t) * (nsub + 1), "box offsets");
+	if (s == CT_OK) {
+		s = dalloc(c, (void**) &b->d_sub_sums, sizeof(double) * 9 * nsub, "box sums");
+	}
+	if (s == CT_OK) {
+		s = dalloc(c, (void**) &b->d_sub_maxrung, sizeof(int) * nsub, "box max rungs");
+	}
+	if (s == CT_OK && cudaMemcpy(b->d_sub_off, b->sub_off.data(), sizeof(int64_t) * (nsub + 1), cudaMemcpyHostToDevice) != cudaSuccess) {
+		s = fail(c, CT_ERR_CUDA, "copy of box offsets");
+	}
 	for (int d = 0; d < 3 && s == CT_OK; d++) {
 		s = dalloc(c, (void**) &b->x[d], sizeof(uint32_t) * n, "positions");
 		if (s == CT_OK) {
@@ -590,6 +610,9 @@ ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id) {
 			dfree(c, b->x[d], sizeof(uint32_t) * n);
 			dfree(c, b->v[d], sizeof(float) * n);
 		}
+		dfree(c, b->d_sub_off, sizeof(int64_t) * (nsub + 1));
+		dfree(c, b->d_sub_sums, sizeof(double) * 9 * nsub);
+		dfree(c, b->d_sub_maxrung, sizeof(int) * nsub);
 		delete b;
 		return s;
 	}
@@ -607,6 +630,49 @@ ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id) {
 	c->boxes[id] = b;
 	*box_id = id;
 	return CT_OK;
+}
+
+ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c || n < 0 || !box_id) {
+		return fail(c, CT_ERR_ARG, "ct_box_create: bad arguments");
+	}
+	return box_create_impl(c, 1, &n, box_id);
+}
+
+ct_status ct_ensemble_create(ct_ctx* ctx, int nbox, const int64_t* counts, int* box_id) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c || nbox < 1 || !counts || !box_id) {
+		return fail(c, CT_ERR_ARG, "ct_ensemble_create: bad arguments");
+	}
+	return box_create_impl(c, nbox, counts, box_id);
+}
+
+ct_status ct_ensemble_set_params(ct_ctx* ctx, int box_id, const float* h, const float* GM) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !h || !GM) {
+		return fail(c, CT_ERR_ARG, "ct_ensemble_set_params: bad arguments");
+	}
+	for (int s = 0; s < b->nsub; s++) {
+		if (!(h[s] > 0.f) || !(GM[s] > 0.f)) {
+			return fail(c, CT_ERR_ARG, "ct_ensemble_set_params: softening and GM must be positive");
+		}
+	}
+	cudaSetDevice(c->device);
+	if (!b->d_sub_h) {
+		CT_TRY(dalloc(c, (void**) &b->d_sub_h, sizeof(float) * b->nsub, "box softening"));
+		CT_TRY(dalloc(c, (void**) &b->d_sub_GM, sizeof(float) * b->nsub, "box GM"));
+	}
+	b->sub_h_host.assign(h, h + b->nsub);
+	CT_CUDA(c, cudaMemcpy(b->d_sub_h, h, sizeof(float) * b->nsub, cudaMemcpyHostToDevice));
+	CT_CUDA(c, cudaMemcpy(b->d_sub_GM, GM, sizeof(float) * b->nsub, cudaMemcpyHostToDevice));
+	return CT_OK;
+}
+
+int ct_box_count(const ct_ctx* ctx, int box_id) {
+	Box* b = get_box((Ctx*) ctx, box_id);
+	return b ? b->nsub : -1;
 }
 
 ct_status ct_box_destroy(ct_ctx* ctx, int box_id) {
@@ -633,6 +699,11 @@ ct_status ct_box_destroy(ct_ctx* ctx, int box_id) {
 	dfree(c, b->parent, sizeof(int32_t) * cap);
 	dfree(c, b->gbox, sizeof(double) * 6 * cap);
 	dfree(c, b->tbox, sizeof(double) * 6 * cap);
+	dfree(c, b->d_sub_off, sizeof(int64_t) * (b->nsub + 1));
+	dfree(c, b->d_sub_sums, sizeof(double) * 9 * b->nsub);
+	dfree(c, b->d_sub_maxrung, sizeof(int) * b->nsub);
+	dfree(c, b->d_sub_h, sizeof(float) * b->nsub);
+	dfree(c, b->d_sub_GM, sizeof(float) * b->nsub);
 	delete b;
 	c->boxes[box_id] = nullptr;
 	return CT_OK;
@@ -755,6 +826,9 @@ ct_status ct_sort_by_rung(ct_ctx* ctx, int box_id, int min_rung, int64_t* rung_b
 	if (!b || min_rung < 0 || min_rung > 15) {
 		return fail(c, CT_ERR_ARG, "ct_sort_by_rung: bad arguments");
 	}
+	if (b->nsub > 1 && min_rung > 0) {
+		return fail(c, CT_ERR_ARG, "ct_sort_by_rung: an ensemble is kicked with all particles active (min_rung 0)");
+	}
 	cudaSetDevice(c->device);
 	CT_TRY(sort_by_rung_run(c, b, min_rung));
 	if (rung_begin) {
@@ -803,6 +877,38 @@ ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick
 		CT_TRY(dalloc(c, (void**) &b->pot, sizeof(float) * b->n, "potentials"));
 	}
 	return kick_run(c, b, params, result);
+}
+
+ct_status ct_kick_ensemble(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* results) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !results) {
+		return fail(c, CT_ERR_ARG, "ct_kick_ensemble: bad arguments");
+	}
+	ct_kick_return total;
+	CT_TRY(ct_kick(ctx, box_id, params, &total));
+	if (b->nsub == 1) {
+		results[0] = total;
+		return CT_OK;
+	}
+	std::vector<double> sums(9 * b->nsub);
+	std::vector<int> mr(b->nsub);
+	CT_CUDA(c, cudaMemcpyAsync(sums.data(), b->d_sub_sums, sizeof(double) * 9 * b->nsub, cudaMemcpyDeviceToHost, c->stream));
+	CT_CUDA(c, cudaMemcpyAsync(mr.data(), b->d_sub_maxrung, sizeof(int) * b->nsub, cudaMemcpyDeviceToHost, c->stream));
+	CT_CUDA(c, cudaStreamSynchronize(c->stream));
+	for (int s = 0; s < b->nsub; s++) {
+		ct_kick_return& r = results[s];
+		const double* q = sums.data() + 9 * s;
+		r.pot = q[0];
+		r.kin = q[1];
+		r.dkin = q[2];
+		r.xmom = q[3];
+		r.ymom = q[4];
+		r.zmom = q[5];
+		r.nmom = q[6];
+		r.max_rung = mr[s];
+	}
+	return CT_OK;
 }
 
 ct_status ct_drift(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag) {

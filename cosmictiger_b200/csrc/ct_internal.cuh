@@ -26,6 +26,20 @@ struct __align__(16) NodeW {
 	int32_t flags;       // bit 0: leaf
 };
 
+// Box of an ensemble that owns particle index p (sub_off has nsub + 1 entries).
+__host__ __device__ inline int box_of(const int64_t* sub_off, int nsub, int64_t p) {
+	int lo = 0, hi = nsub - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (sub_off[mid] <= p) {
+			lo = mid;
+		} else {
+			hi = mid - 1;
+		}
+	}
+	return lo;
+}
+
 // fixed32 helpers (cosmictiger/fixed.hpp)
 __host__ __device__ inline float fixed_dist(uint32_t a, uint32_t b) {
 	return float(int32_t(a - b)) * (1.0f / 4294967296.0f);
@@ -83,6 +97,16 @@ struct Box {
 	double* multi_d = nullptr;  // multipole in double before rounding, NMULT_STRIDE per node
 	bool tree_valid = false;
 	ct_tree_params tparams;
+	// ensemble: nsub independent periodic unit boxes stored back to back; sub-box s owns
+	// particles [sub_off[s], sub_off[s+1]) and tree root node s
+	int nsub = 1;
+	std::vector<int64_t> sub_off;
+	int64_t* d_sub_off = nullptr;
+	double* d_sub_sums = nullptr;  // 9 kick sums per sub-box
+	int* d_sub_maxrung = nullptr;
+	float* d_sub_h = nullptr;      // per-box softening (null: the kick's h for all)
+	float* d_sub_GM = nullptr;     // per-box GM (null: the kick's GM for all)
+	std::vector<float> sub_h_host;
 	// kick results
 	ct_counters counters;
 	bool have_force = false;

@@ -101,7 +101,9 @@ struct WalkOut {
 struct WalkParams {
 	float thetainv;
 	float h;
-	int level0;
+	int nroot;  // nodes [0, nroot) are the roots of independent boxes
+	const int64_t* sub_off;
+	const float* sub_h;  // per-box softening of an ensemble, or null
 };
 
 __device__ __forceinline__ float sqrf3(float a, float b, float c) {
@@ -188,9 +190,10 @@ __global__ void __launch_bounds__(WALK_TPB) k_walk(int64_t lb, int64_t le, const
 		sl[k] = st + k * cap;
 	}
 	int ovf = 0, dropped = 0;
-	const float thetainv = p.thetainv, h = p.h;
+	const float thetainv = p.thetainv;
 	for (int64_t si = lb + gw; si < le; si += nw) {
 		const NodeW self = nodes[si];
+		const float h = p.sub_h ? p.sub_h[box_of(p.sub_off, p.nroot, self.pbeg)] : p.h;
 		const int nsinks = self.pend - self.pbeg;
 		const bool sleaf = self.flags & 1;
 		int2 z2 = make_int2(0, 0);
@@ -213,8 +216,8 @@ __global__ void __launch_bounds__(WALK_TPB) k_walk(int64_t lb, int64_t le, const
 		const int* ein;
 		const int* din;
 		int ne, nd;
-		int root_list = 0;
-		if (si == 0) {
+		int root_list = (int) si;
+		if (si < p.nroot) {
 			ein = din = &root_list;
 			ne = nd = 1;
 		} else {
@@ -530,7 +533,7 @@ __global__ void k_l2l(int64_t lb, int64_t le, const NodeW* __restrict__ nodes, c
 	for (int64_t i = lb + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < le; i += (int64_t) gridDim.x * blockDim.x) {
 		float out[NE];
 		const float* d = dL + NEXP_STRIDE * i;
-		if (i == 0) {
+		if (parent[i] < 0) {  // a root: the expansion starts at zero
 			for (int k = 0; k < NE; k++) {
 				out[k] = d[k];
 			}
@@ -832,6 +835,9 @@ constexpr int P2P_TPB = 256;
 constexpr int P2P_STAGE = 64;
 
 struct P2PArgs {
+	int nsub;
+	const int64_t* sub_off;
+	const float* sub_h;
 	const NodeW* nodes;
 	const int2* items;  // (leaf node, tile)
 	int64_t nitems;
@@ -850,11 +856,12 @@ __global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
 	float4* my = stage[w];
-	const float h = a.h, h2 = h * h, hinv = 1.f / h, h2inv = hinv * hinv, h3inv = h2inv * hinv;
 	double npairs = 0.0;
 	for (int64_t it = gw; it < a.nitems; it += nw) {
 		const int2 item = a.items[it];
 		const NodeW self = a.nodes[item.x];
+		const float h = a.sub_h ? a.sub_h[box_of(a.sub_off, a.nsub, self.pbeg)] : a.h;
+		const float h2 = h * h, hinv = 1.f / h, h2inv = hinv * hinv, h3inv = h2inv * hinv;
 		const int k = self.pbeg + 32 * item.y + lane;
 		const bool active = k < self.pend;
 		float kx = 0.f, ky = 0.f, kz = 0.f;
@@ -936,6 +943,12 @@ __global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
 }
 
 struct KickTileArgs {
+	int nsub;               // > 1: per-box sums for an ensemble
+	const int64_t* sub_off; // particle offsets of the boxes (nsub + 1)
+	double* sub_sums;       // 9 per box
+	int* sub_maxrung;
+	const float* sub_h;
+	const float* sub_GM;
 	const NodeW* nodes;
 	const float* multi;
 	const float* Lx;
@@ -955,6 +968,8 @@ struct KickTileArgs {
 };
 
 // M2P, L2P and the kick for one 32-sink tile per warp (gravity.cu:157-211, kick.cu:53-177).
+// Sums of the kick return go to one set per box: block-reduced for a single box, per tile
+// (warp-reduced, atomically added to the tile's box) for an ensemble.
 template<class Ops>
 __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
@@ -963,7 +978,6 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
 	const auto& kp = a.kp;
-	const float hinv = 1.f / kp.h;
 	double acc[9];
 	for (int q = 0; q < 9; q++) {
 		acc[q] = 0.0;
@@ -972,6 +986,10 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 	for (int64_t it = gw; it < a.nitems; it += nw) {
 		const int2 item = a.items[it];
 		const NodeW self = a.nodes[item.x];
+		const int bx = a.nsub > 1 ? box_of(a.sub_off, a.nsub, self.pbeg) : 0;
+		const float hh = a.sub_h ? a.sub_h[bx] : kp.h;
+		const float GM = a.sub_GM ? a.sub_GM[bx] : kp.GM;
+		const float hinv = 1.f / hh;
 		const int k = self.pbeg + 32 * item.y + lane;
 		const bool active = k < self.pend;
 		uint32_t X[3] = { self.x, self.y, self.z };
@@ -997,72 +1015,97 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 			Fz -= 1e6f * L2[3];
 			Fp += 1e3f * L2[0];
 		}
-		if (!active) {
-			continue;
+		double ia[9];
+		for (int q = 0; q < 9; q++) {
+			ia[q] = 0.0;
 		}
-		acc[8] += pcl.y;
-		const float4 P = a.F[k];
-		Fx -= P.x;
-		Fy -= P.y;
-		Fz -= P.z;
-		Fp += P.w;
-		float La[NE], L2[5];
-		const float* Lsrc = a.Lx + (size_t) NEXP_STRIDE * item.x;
-		for (int i = 0; i < NE; i++) {
-			La[i] = Lsrc[i];
-		}
-		Ops::l2p(L2, La, fixed_dist(X[0], self.x), fixed_dist(X[1], self.y), fixed_dist(X[2], self.z), kp.do_phi != 0);
-		Fp += 1e3f * L2[0];
-		Fx -= 1e6f * L2[1];
-		Fy -= 1e6f * L2[2];
-		Fz -= 1e6f * L2[3];
-		Fz *= kp.GM;
-		Fy *= kp.GM;
-		Fx *= kp.GM;
-		Fp *= kp.GM;
-		float vx = a.v[0][k], vy = a.v[1][k], vz = a.v[2][k];
-		const float kin0 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
-		const float sgn = kp.sign * (kp.top ? 1.f : -1.f);
-		const float rdt = 1.0f / (float) (1 << kp.min_rung);
-		if (kp.ascending) {
-			const float dt = 0.5f * rdt * kp.t0;
-			if (!kp.first_call) {
+		int imax = 0;
+		if (active) {
+			ia[8] = pcl.y;
+			const float4 P = a.F[k];
+			Fx -= P.x;
+			Fy -= P.y;
+			Fz -= P.z;
+			Fp += P.w;
+			float La[NE], L2[5];
+			const float* Lsrc = a.Lx + (size_t) NEXP_STRIDE * item.x;
+			for (int i = 0; i < NE; i++) {
+				La[i] = Lsrc[i];
+			}
+			Ops::l2p(L2, La, fixed_dist(X[0], self.x), fixed_dist(X[1], self.y), fixed_dist(X[2], self.z), kp.do_phi != 0);
+			Fp += 1e3f * L2[0];
+			Fx -= 1e6f * L2[1];
+			Fy -= 1e6f * L2[2];
+			Fz -= 1e6f * L2[3];
+			Fz *= GM;
+			Fy *= GM;
+			Fx *= GM;
+			Fp *= GM;
+			float vx = a.v[0][k], vy = a.v[1][k], vz = a.v[2][k];
+			const float kin0 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
+			const float sgn = kp.sign * (kp.top ? 1.f : -1.f);
+			const float rdt = 1.0f / (float) (1 << kp.min_rung);
+			if (kp.ascending) {
+				const float dt = 0.5f * rdt * kp.t0;
+				if (!kp.first_call) {
+					vx = fmaf(sgn * Fx, dt, vx);
+					vy = fmaf(sgn * Fy, dt, vy);
+					vz = fmaf(sgn * Fz, dt, vz);
+				}
+			}
+			ia[1] = 0.5f * (vx * vx + vy * vy + vz * vz);
+			ia[3] = vx;
+			ia[4] = vy;
+			ia[5] = vz;
+			ia[6] = sqrtf(vx * vx + vy * vy + vz * vz);
+			if (kp.save_force) {
+				a.g[0][k] = Fx;
+				a.g[1][k] = Fy;
+				a.g[2][k] = Fz;
+				a.pot[k] = Fp;
+			}
+			if (kp.descending) {
+				const float g2 = Fx * Fx + Fy * Fy + Fz * Fz;
+				float dt = fminf(kp.eta * sqrtf(kp.a * hh * rsqrtf(g2)), kp.t0);
+				dt = fminf(kp.max_dt, dt);
+				int r = a.rung[k];
+				r = max(kp.min_rung + int((int) ceilf(log2f(kp.t0 / dt)) > kp.min_rung), r - 1);
+				r = max(0, min(r, 15));
+				a.rung[k] = (int8_t) r;
+				imax = r;
+				dt = 0.5f * rdt * kp.t0;
 				vx = fmaf(sgn * Fx, dt, vx);
 				vy = fmaf(sgn * Fy, dt, vy);
 				vz = fmaf(sgn * Fz, dt, vz);
 			}
+			const float kin1 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
+			a.v[0][k] = vx;
+			a.v[1][k] = vy;
+			a.v[2][k] = vz;
+			ia[0] = 0.5f * Fp;
+			ia[2] = kin1 - kin0;
 		}
-		acc[1] += 0.5f * (vx * vx + vy * vy + vz * vz);
-		acc[3] += vx;
-		acc[4] += vy;
-		acc[5] += vz;
-		acc[6] += sqrtf(vx * vx + vy * vy + vz * vz);
-		if (kp.save_force) {
-			a.g[0][k] = Fx;
-			a.g[1][k] = Fy;
-			a.g[2][k] = Fz;
-			a.pot[k] = Fp;
+		if (a.nsub > 1) {
+			for (int q = 0; q < 9; q++) {
+				for (int o = 16; o; o >>= 1) {
+					ia[q] += __shfl_xor_sync(0xffffffffu, ia[q], o);
+				}
+			}
+			for (int o = 16; o; o >>= 1) {
+				imax = max(imax, __shfl_xor_sync(0xffffffffu, imax, o));
+			}
+			if (lane == 0) {
+				const int lo = bx;
+				for (int q = 0; q < 9; q++) {
+					atomicAdd(a.sub_sums + 9 * lo + q, ia[q]);
+				}
+				atomicMax(a.sub_maxrung + lo, imax);
+			}
 		}
-		if (kp.descending) {
-			const float g2 = Fx * Fx + Fy * Fy + Fz * Fz;
-			float dt = fminf(kp.eta * sqrtf(kp.a * kp.h * rsqrtf(g2)), kp.t0);
-			dt = fminf(kp.max_dt, dt);
-			int r = a.rung[k];
-			r = max(kp.min_rung + int((int) ceilf(log2f(kp.t0 / dt)) > kp.min_rung), r - 1);
-			r = max(0, min(r, 15));
-			a.rung[k] = (int8_t) r;
-			maxr = max(maxr, r);
-			dt = 0.5f * rdt * kp.t0;
-			vx = fmaf(sgn * Fx, dt, vx);
-			vy = fmaf(sgn * Fy, dt, vy);
-			vz = fmaf(sgn * Fz, dt, vz);
+		for (int q = 0; q < 9; q++) {
+			acc[q] += ia[q];
 		}
-		const float kin1 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
-		a.v[0][k] = vx;
-		a.v[1][k] = vy;
-		a.v[2][k] = vz;
-		acc[0] += 0.5f * Fp;
-		acc[2] += kin1 - kin0;
+		maxr = max(maxr, imax);
 	}
 	for (int q = 0; q < 9; q++) {
 		double v = acc[q];
@@ -1218,6 +1261,9 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		WalkParams wp;
 		wp.thetainv = 1.f / kp->theta;
 		wp.h = kp->h;
+		wp.nroot = b->nsub;
+		wp.sub_off = b->d_sub_off;
+		wp.sub_h = b->d_sub_h;
 		cudaEventRecord(c->ev[0], st);
 		const int nlev = (int) b->level_start.size() - 1;
 		for (int k = 0; k < nlev; k++) {
@@ -1291,7 +1337,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		la.compensated = 1;
 		la.sums = counters + 4;
 		la.max_rung = c->d_flags + 48;
-		static const bool fused = getenv("CT_LEAF_FUSED") != nullptr;
+		const bool fused = getenv("CT_LEAF_FUSED") != nullptr && b->nsub == 1 && !b->d_sub_h;
 		if (fused) {
 			cudaEventRecord(c->ev[4], st);
 			if (nleaves > 0) {
@@ -1322,6 +1368,9 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			c->launches++;
 			k_tile_fill<<<(int) std::max<int64_t>(1, std::min<int64_t>((nleaves + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nleaves, K.leaves, ntl, off, items);
 			P2PArgs pa;
+			pa.nsub = b->nsub;
+			pa.sub_off = b->d_sub_off;
+			pa.sub_h = b->d_sub_h;
 			pa.nodes = b->nodes;
 			pa.items = items;
 			pa.nitems = nitems;
@@ -1339,6 +1388,16 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			k_p2p<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
 			cudaEventRecord(c->ev[5], st);
 			KickTileArgs ka;
+			ka.nsub = b->nsub;
+			ka.sub_off = b->d_sub_off;
+			ka.sub_sums = b->d_sub_sums;
+			ka.sub_maxrung = b->d_sub_maxrung;
+			ka.sub_h = b->d_sub_h;
+			ka.sub_GM = b->d_sub_GM;
+			if (b->nsub > 1) {
+				CT_CUDA(c, cudaMemsetAsync(b->d_sub_sums, 0, sizeof(double) * 9 * b->nsub, st));
+				CT_CUDA(c, cudaMemsetAsync(b->d_sub_maxrung, 0, sizeof(int) * b->nsub, st));
+			}
 			ka.nodes = b->nodes;
 			ka.multi = b->multi;
 			ka.Lx = K.Lx;

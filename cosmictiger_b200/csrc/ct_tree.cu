@@ -94,22 +94,29 @@ __device__ __forceinline__ int block_excl_scan(int v, int* sh, int* total) {
 	return base + inc - v;
 }
 
-__global__ void k_init_root(NodeW* nodes, double* gbox, uint64_t* key, int32_t* depth, int32_t* parent, int32_t pbeg, int32_t pend) {
+// One root per sub-box: node s covers the unit box and particles [off[s], off[s+1]), except
+// that a single box starts at the active range [pbeg, pend).
+__global__ void k_init_roots(int nroot, const int64_t* off, NodeW* nodes, double* gbox, uint64_t* key, int32_t* depth, int32_t* parent, int32_t pbeg,
+		int32_t pend) {
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if (s >= nroot) {
+		return;
+	}
 	NodeW r;
 	r.x = r.y = r.z = 0;
 	r.radius = 0.f;
-	r.pbeg = pbeg;
-	r.pend = pend;
+	r.pbeg = nroot == 1 ? pbeg : (int32_t) off[s];
+	r.pend = nroot == 1 ? pend : (int32_t) off[s + 1];
 	r.child = -1;
 	r.flags = 1;
-	nodes[0] = r;
+	nodes[s] = r;
 	for (int d = 0; d < 3; d++) {
-		gbox[d] = 0.0;
-		gbox[3 + d] = 1.0;
+		gbox[6 * s + d] = 0.0;
+		gbox[6 * s + 3 + d] = 1.0;
 	}
-	key[0] = 1;
-	depth[0] = 0;
-	parent[0] = -1;
+	key[s] = 1;
+	depth[s] = 0;
+	parent[s] = -1;
 }
 
 __global__ void k_iota(int32_t* idx, int64_t n) {
@@ -782,11 +789,13 @@ ct_status tree_build_t(Ctx* c, Box* b, const ct_tree_params* p) {
 	c->launches++;
 	k_iota<<<grid_for(c, n, 256), 256, 0, st>>>(s.idx, n);
 	c->launches++;
-	k_init_root<<<1, 1, 0, st>>>(b->nodes, b->gbox, b->key, b->depth, b->parent, (int32_t) pb, (int32_t) n);
+	const int nroot = b->nsub;
+	CT_TRY(ensure_nodes(c, b, nroot + 1));
+	k_init_roots<<<(nroot + 127) / 128, 128, 0, st>>>(nroot, b->d_sub_off, b->nodes, b->gbox, b->key, b->depth, b->parent, (int32_t) pb, (int32_t) n);
 	CT_CUDA(c, cudaMemsetAsync(c->d_flags, 0, 4 * sizeof(int), st));
 	std::vector<int64_t> levels;
 	levels.push_back(0);
-	int64_t lb = 0, le = 1;
+	int64_t lb = 0, le = nroot;
 	int32_t* h_tot = (int32_t*) c->pinned;
 	while (le > lb) {
 		levels.push_back(le);

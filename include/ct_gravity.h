@@ -120,6 +120,19 @@ ct_status ct_box_create(ct_ctx* ctx, int64_t n, int* box_id);
 ct_status ct_box_destroy(ct_ctx* ctx, int box_id);
 int64_t ct_box_size(const ct_ctx* ctx, int box_id);
 
+/* An ensemble: nbox independent periodic unit boxes in one device structure, box s holding
+ * counts[s] particles stored after those of boxes 0..s-1.  Every call on it (tree build, kick,
+ * drift, transfers of the concatenated arrays) covers all boxes with one set of kernel
+ * launches; the boxes never interact.  Kicked with all particles active (min_rung 0). */
+ct_status ct_ensemble_create(ct_ctx* ctx, int nbox, const int64_t* counts, int* box_id);
+/* Per-box softening h and GM of an ensemble (box s: h[s], GM[s]); without this call every box
+ * uses the kick's h and GM.  The tree build's leaf criterion uses the tree parameters' hsoft. */
+ct_status ct_ensemble_set_params(ct_ctx* ctx, int box_id, const float* h, const float* GM);
+/* Number of boxes of an ensemble (1 for a plain box). */
+int ct_box_count(const ct_ctx* ctx, int box_id);
+/* Kick of every box of an ensemble; results[s] receives box s's kick_return. */
+ct_status ct_kick_ensemble(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* results);
+
 /* Host <-> device transfers.  x,y,z: fixed32 positions (uint32, 2^-32 box units);
  * vxyz: float[3*n] interleaved velocities (the reference's particles_v layout);
  * rung: int8[n].  Download arguments may be NULL to skip a field; g/pot only exist after a

@@ -113,9 +113,21 @@ def test_tree_bitexact(ctx, oracle, n, theta, bucket, seed):
     box.close()
 
 
-@pytest.mark.parametrize("n,theta,seed", [(16, 0.7, 1), (24, 0.55, 4)])
-def test_kick_parity(ctx, oracle, n, theta, seed):
-    x, y, z, v, r = lattice(n, seed=seed)
+# Potentials of a periodic box are small residuals of two large sums (the softened direct
+# part, about -2.38 GM N per particle for a near-uniform box, and the Ewald correction,
+# about +2.38 GM N): float rounding in either sum appears in the residual amplified by
+# 100-300x.  Potentials are therefore compared relative to that scale (POT_SCALE_TOL), and
+# by plain relative RMS only where the potential wells are deep (clustered input).
+POT_SCALE_TOL = 1e-6
+MEAN_INV_R_UNIT_CELL = 2.3800772  # integral of 1/|x| over the unit cell
+
+
+@pytest.mark.parametrize("n,theta,seed,kind", [(16, 0.7, 1, "lattice"), (24, 0.55, 4, "lattice"), (24, 0.55, 5, "clustered")])
+def test_kick_parity(ctx, oracle, n, theta, seed, kind):
+    if kind == "clustered":
+        x, y, z, v, r = ics.clustered_box(n, nspheres=40, seed=seed)
+    else:
+        x, y, z, v, r = lattice(n, seed=seed)
     N = len(x)
     h = ics.softening(N, 0.02)
     box = ctx.box(N)
@@ -129,14 +141,20 @@ def test_kick_parity(ctx, oracle, n, theta, seed):
     g_gpu = np.stack([out["gx"], out["gy"], out["gz"]], 1).astype(np.float64)
     g_or = np.stack([gx, gy, gz], 1).astype(np.float64)
     err = rel_rms(g_gpu, g_or)
+    dphi = out["pot"].astype(np.float64) - pot.astype(np.float64)
     perr = rel_rms(out["pot"].astype(np.float64), pot.astype(np.float64))
+    pscale = float(np.sqrt(np.mean(dphi ** 2))) / (MEAN_INV_R_UNIT_CELL * (1.0 / N) * N)
+    print("kick parity %s n=%d theta=%g: force rel rms %.3g, potential rel rms %.3g, potential / scale %.3g" % (kind, n, theta, err, perr, pscale))
     assert err < KICK_RMS_TOL, err
-    assert perr < KICK_RMS_TOL, perr
+    assert pscale < POT_SCALE_TOL, pscale
+    if kind == "clustered":
+        assert perr < KICK_RMS_TOL, perr
     # velocities after the kick and rungs
     assert rel_rms(out["v"].astype(np.float64), ov.astype(np.float64)) < KICK_RMS_TOL
     assert np.mean(out["rung"] != orr) < 1e-3
     assert kr.max_rung == orc.max_rung
-    assert abs(kr.pot - orc.pot) <= 1e-5 * abs(orc.pot)
+    # the potential energy sum carries the same cancellation (scale: N/2 potentials)
+    assert abs(kr.pot - orc.pot) <= POT_SCALE_TOL * 0.5 * MEAN_INV_R_UNIT_CELL * N
     assert abs(kr.kin - orc.kin) <= 1e-5 * abs(orc.kin)
     box.close()
 
@@ -173,3 +191,37 @@ def test_force_accuracy_vs_direct_ewald(ctx):
     err = np.linalg.norm(g_t - g_d, axis=1) / np.linalg.norm(g_d, axis=1)
     assert np.sqrt(np.mean(err ** 2)) < 3e-3
     box.close()
+
+
+def test_ensemble_matches_separate_boxes(ctx):
+    """Boxes run as one ensemble, each with its own softening and GM, give bit-identical
+    trees and forces to the same boxes run one by one (the boxes never interact; every kernel
+    treats them independently)."""
+    sets = [lattice(12, seed=21), ics.clustered_box(10, nspheres=5, seed=22), lattice(14, seed=23, index=-1.5, rms=0.5)]
+    theta = 0.55
+    counts = [len(s[0]) for s in sets]
+    h = [ics.softening(n, 0.02) for n in counts]
+    # the ensemble uses one softening; give every box the same h for the comparison
+    hh = min(h)
+    gms = [1.0 / n for n in counts]
+    ens = ctx.ensemble(counts)
+    cat = [np.concatenate([s[k] for s in sets]) for k in range(5)]
+    ens.upload(*cat)
+    ens.set_box_params(h, gms)
+    ens.tree_create(theta, hh, 128)
+    krs = ens.kick_ensemble(kick_params(theta, hh, 1000))
+    eo = ens.download(forces=True)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for s, st in enumerate(sets):
+        b = ctx.box(counts[s])
+        b.upload(*st)
+        b.tree_create(theta, hh, 128)
+        kr = b.kick(kick_params(theta, h[s], counts[s]))
+        o = b.download(forces=True)
+        sl = slice(off[s], off[s + 1])
+        for f in ("x", "y", "z", "v", "rung", "gx", "gy", "gz", "pot"):
+            assert np.array_equal(eo[f][sl], o[f]), (s, f)
+        assert krs[s].max_rung == kr.max_rung
+        assert abs(krs[s].kin - kr.kin) <= 1e-9 * abs(kr.kin)
+        b.close()
+    ens.close()
