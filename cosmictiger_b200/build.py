@@ -21,6 +21,7 @@ UNITS = {
     "ct_tree.cu": ["-fmad=false"],
     "ct_kick.cu": ["-fmad=false"],
     "ct_api.cu": [],
+    "ct_noalloc.cu": [],
 }
 
 

@@ -175,6 +175,29 @@ ct_status ct_fp32_peak(ct_ctx* ctx, double* tflops);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own work with it. */
 void* ct_stream(ct_ctx* ctx);
 
+/* ---- allocation-free variant (no counterpart in the reference)
+ *
+ * For callers that cannot allocate device memory when they partition rungs: a host driver
+ * living inside a memory pool it does not own, an embedding application whose allocator
+ * forbids cudaMalloc/cudaFree on its hot path, or code that must keep its device footprint
+ * fixed after start-up.  Same result as ct_sort_by_rung (particles with rung < min_rung move to
+ * [begin, *rung_begin), the rest to [*rung_begin, n), with the reference's exact two-pointer
+ * permutation), but on device arrays the caller already holds (SoA velocities), on the
+ * caller's stream, with no context and no allocation: all temporary storage is one
+ * file-scope __device__ array of fixed size that every GPU loading the library keeps until
+ * process exit (about 17 MB).
+ *   - at most CT_NOALLOC_MAX_PARTICLES particles in [begin, n); more returns CT_ERR_CAPACITY
+ *     (and a message on stderr) before any device work;
+ *   - the first call on each device looks up the array's device address; make that first call
+ *     before any stream capture;
+ *   - every call shares the one array: calls that overlap on the GPU (other streams, other
+ *     host threads) race and must be serialised by the caller;
+ *   - min_rung == 0 resets *rung_begin to 0 without touching the arrays, like the reference.
+ * Returns after synchronising `stream` (a cudaStream_t; NULL is the legacy default stream). */
+#define CT_NOALLOC_MAX_PARTICLES (1 << 20)
+ct_status ct_sort_by_rung_noalloc(int64_t begin, int64_t n, int min_rung, uint32_t* x, uint32_t* y, uint32_t* z, float* vx, float* vy, float* vz,
+		int8_t* rung, int64_t* rung_begin, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
