@@ -850,6 +850,29 @@ struct P2PArgs {
 	double* pairs;
 };
 
+// r^-1 and r^-3 of a pair, or the Ferrer-softened values inside h (gravity.hpp:73-96).
+__device__ __forceinline__ void pair_kernel(float r2, float h2, float hinv, float h2inv, float h3inv, float& r1inv, float& r3inv) {
+	if (r2 > h2) {
+		r1inv = rsqrtf(r2);
+		r3inv = r1inv * r1inv * r1inv;
+	} else {
+		const float q2 = r2 * h2inv;
+		float f = 315.f / 128.f;
+		f = fmaf(f, q2, -385.f / 32.f);
+		f = fmaf(f, q2, 1485.f / 64.f);
+		f = fmaf(f, q2, -693.f / 32.f);
+		f = fmaf(f, q2, 1155.f / 128.f);
+		r3inv = f * h3inv;
+		float ph = -63.f / 256.f;
+		ph = fmaf(ph, q2, 385.f / 256.f);
+		ph = fmaf(ph, q2, -495.f / 128.f);
+		ph = fmaf(ph, q2, 693.f / 128.f);
+		ph = fmaf(ph, q2, -1155.f / 256.f);
+		ph = fmaf(ph, q2, 693.f / 256.f);
+		r1inv = ph * hinv;
+	}
+}
+
 __global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
 	__shared__ float4 stage[P2P_TPB / 32][P2P_STAGE];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -882,38 +905,52 @@ __global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
 					my[j] = make_float4(fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z), 0.f);
 				}
 				__syncwarp();
+				// two sources per iteration with separate accumulators; the softened kernel runs
+				// only when some lane of the warp has a pair inside h (warp-uniform branch)
 				float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
-#pragma unroll 4
-				for (int j = 0; j < cnt; j++) {
-					const float4 s = my[j];
-					const float dx = kx - s.x, dy = ky - s.y, dz = kz - s.z;
-					const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-					float r1inv, r3inv;
-					if (r2 > h2) {
-						r1inv = rsqrtf(r2);
-						r3inv = r1inv * r1inv * r1inv;
+				float gx = 0.f, gy = 0.f, gz = 0.f, qt = 0.f;
+				int j = 0;
+				for (; j + 1 < cnt; j += 2) {
+					const float4 s0 = my[j];
+					const float4 s1 = my[j + 1];
+					const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
+					const float dx1 = kx - s1.x, dy1 = ky - s1.y, dz1 = kz - s1.z;
+					const float r20 = fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0));
+					const float r21 = fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1));
+					float r1a, r3a, r1b, r3b;
+					if (__any_sync(0xffffffffu, fminf(r20, r21) <= h2)) {
+						pair_kernel(r20, h2, hinv, h2inv, h3inv, r1a, r3a);
+						pair_kernel(r21, h2, hinv, h2inv, h3inv, r1b, r3b);
 					} else {
-						// Ferrer softening kernel (gravity.hpp:73-96)
-						const float q2 = r2 * h2inv;
-						float f = 315.f / 128.f;
-						f = fmaf(f, q2, -385.f / 32.f);
-						f = fmaf(f, q2, 1485.f / 64.f);
-						f = fmaf(f, q2, -693.f / 32.f);
-						f = fmaf(f, q2, 1155.f / 128.f);
-						r3inv = f * h3inv;
-						float ph = -63.f / 256.f;
-						ph = fmaf(ph, q2, 385.f / 256.f);
-						ph = fmaf(ph, q2, -495.f / 128.f);
-						ph = fmaf(ph, q2, 693.f / 128.f);
-						ph = fmaf(ph, q2, -1155.f / 256.f);
-						ph = fmaf(ph, q2, 693.f / 256.f);
-						r1inv = ph * hinv;
+						r1a = rsqrtf(r20);
+						r3a = r1a * r1a * r1a;
+						r1b = rsqrtf(r21);
+						r3b = r1b * r1b * r1b;
 					}
-					fx = fmaf(dx, r3inv, fx);
-					fy = fmaf(dy, r3inv, fy);
-					fz = fmaf(dz, r3inv, fz);
-					pt -= r1inv;
+					fx = fmaf(dx0, r3a, fx);
+					fy = fmaf(dy0, r3a, fy);
+					fz = fmaf(dz0, r3a, fz);
+					pt -= r1a;
+					gx = fmaf(dx1, r3b, gx);
+					gy = fmaf(dy1, r3b, gy);
+					gz = fmaf(dz1, r3b, gz);
+					qt -= r1b;
 				}
+				if (j < cnt) {
+					const float4 s0 = my[j];
+					const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
+					const float r20 = fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0));
+					float r1a, r3a;
+					pair_kernel(r20, h2, hinv, h2inv, h3inv, r1a, r3a);
+					fx = fmaf(dx0, r3a, fx);
+					fy = fmaf(dy0, r3a, fy);
+					fz = fmaf(dz0, r3a, fz);
+					pt -= r1a;
+				}
+				fx += gx;
+				fy += gy;
+				fz += gz;
+				pt += qt;
 				__syncwarp();
 				if (a.compensated) {
 					ksum(sx, cx, fx);
