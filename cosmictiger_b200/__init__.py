@@ -76,6 +76,20 @@ class TreeParams(ctypes.Structure):
     _fields_ = [("min_rung", ctypes.c_int), ("theta", ctypes.c_double), ("hsoft", ctypes.c_double), ("bucket", ctypes.c_int)]
 
 
+class StepParams(ctypes.Structure):
+    """Parameters of one hierarchical step (kick_step_hierarchical, src/driver.cpp:382)."""
+
+    _fields_ = [("minrung", ctypes.c_int), ("minrung0", ctypes.c_int), ("max_rung", ctypes.c_int), ("a", ctypes.c_double), ("tau", ctypes.c_double),
+                ("t0", ctypes.c_double), ("theta", ctypes.c_double), ("hsoft", ctypes.c_double), ("bucket", ctypes.c_int), ("eta", ctypes.c_float),
+                ("GM", ctypes.c_float), ("max_dt", ctypes.c_float), ("do_phi", ctypes.c_int), ("nocrop", ctypes.c_int), ("drag", ctypes.c_double),
+                ("sign", ctypes.c_float)]
+
+
+class StepReturn(ctypes.Structure):
+    _fields_ = [("kr", KickReturn), ("minrung", ctypes.c_int), ("max_rung", ctypes.c_int), ("particles_kicked", ctypes.c_double), ("kicks", ctypes.c_int),
+                ("particles_drifted_levels", ctypes.c_int)]
+
+
 class Counters(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "pp_pairs", "cc_direct", "cc_ewald", "cp_pairs", "pc_pairs", "nodes", "leaves", "flops", "flops_pp", "flops_cc",
@@ -139,6 +153,8 @@ def library():
     L.ct_box_count.argtypes = [vp, i32]
     L.ct_ensemble_set_params.argtypes = [vp, i32, vp, vp]
     L.ct_kick_ensemble.argtypes = [vp, i32, ctypes.POINTER(KickParams), ctypes.POINTER(KickReturn)]
+    L.ct_step_hierarchical.argtypes = [vp, i32, ctypes.POINTER(StepParams), ctypes.POINTER(StepReturn)]
+    L.ct_rung_counts.argtypes = [vp, i32, vp]
     L.ct_launch_count.argtypes = [vp]
     L.ct_launch_count.restype = ctypes.c_ulonglong
     L.ct_direct_ewald.argtypes = [vp, i32, i64, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
@@ -266,6 +282,17 @@ class Box:
         rc = KickReturn()
         self.ctx.check(self.ctx.lib.ct_kick(self.ctx.h, self.id, ctypes.byref(params), ctypes.byref(rc)), "ct_kick")
         return rc
+
+    def step_hierarchical(self, params):
+        """One multistep step over the rung ladder; returns StepReturn."""
+        r = StepReturn()
+        self.ctx.check(self.ctx.lib.ct_step_hierarchical(self.ctx.h, self.id, ctypes.byref(params), ctypes.byref(r)), "ct_step_hierarchical")
+        return r
+
+    def rung_counts(self):
+        c = np.zeros(16, np.uint64)
+        self.ctx.check(self.ctx.lib.ct_rung_counts(self.ctx.h, self.id, _p(c)), "ct_rung_counts")
+        return c
 
     def drift(self, rung, a, dt, drag=0.0):
         self.ctx.check(self.ctx.lib.ct_drift(self.ctx.h, self.id, rung, a, dt, drag), "ct_drift")

@@ -22,6 +22,7 @@ UNITS = {
     "ct_kick.cu": ["-fmad=false"],
     "ct_api.cu": [],
     "ct_noalloc.cu": [],
+    "ct_driver.cu": [],
 }
 
 

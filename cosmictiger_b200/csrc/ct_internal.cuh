@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -107,6 +108,7 @@ struct Box {
 	float* d_sub_h = nullptr;      // per-box softening (null: the kick's h for all)
 	float* d_sub_GM = nullptr;     // per-box GM (null: the kick's GM for all)
 	std::vector<float> sub_h_host;
+	std::vector<int64_t> rung_stack;  // saved active-range starts (particles_push_rungs)
 	// kick results
 	ct_counters counters;
 	bool have_force = false;
@@ -150,6 +152,8 @@ ct_status kick_run(Ctx* c, Box* b, const ct_kick_params* p, ct_kick_return* out)
 ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag);
 ct_status sort_by_rung_run(Ctx* c, Box* b, int min_rung);
 ct_status ewald_init(Ctx* c);
+ct_status step_hierarchical(Ctx* c, Box* b, const ct_step_params* p, ct_step_return* out);
+ct_status rung_counts(Ctx* c, Box* b, uint64_t* counts);
 ct_status direct_ewald_run(Ctx* c, Box* b, int64_t nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, double h, double* gx,
 		double* gy, double* gz, double* pot);
 

@@ -850,10 +850,18 @@ struct P2PArgs {
 	double* pairs;
 };
 
+// Approximate reciprocal square root (the MUFU unit), flushing denormals: pair separations
+// are at least one fixed32 unit, r^2 >= 2^-64, far above the denormal range.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+	float y;
+	asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+	return y;
+}
+
 // r^-1 and r^-3 of a pair, or the Ferrer-softened values inside h (gravity.hpp:73-96).
 __device__ __forceinline__ void pair_kernel(float r2, float h2, float hinv, float h2inv, float h3inv, float& r1inv, float& r3inv) {
 	if (r2 > h2) {
-		r1inv = rsqrtf(r2);
+		r1inv = rsqrt_ftz(r2);
 		r3inv = r1inv * r1inv * r1inv;
 	} else {
 		const float q2 = r2 * h2inv;
@@ -922,9 +930,9 @@ __global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
 						pair_kernel(r20, h2, hinv, h2inv, h3inv, r1a, r3a);
 						pair_kernel(r21, h2, hinv, h2inv, h3inv, r1b, r3b);
 					} else {
-						r1a = rsqrtf(r20);
+						r1a = rsqrt_ftz(r20);
 						r3a = r1a * r1a * r1a;
-						r1b = rsqrtf(r21);
+						r1b = rsqrt_ftz(r21);
 						r3b = r1b * r1b * r1b;
 					}
 					fx = fmaf(dx0, r3a, fx);

@@ -153,6 +153,39 @@ ct_status ct_tree_create(ct_ctx* ctx, int box_id, const ct_tree_params* params, 
 ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* result);
 ct_status ct_drift(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag);
 
+/* ---- hierarchical (multistep) step: kick_step_hierarchical (src/driver.cpp:382-593) */
+typedef struct {
+	int minrung;      /* the step's minimum rung */
+	int minrung0;     /* the run's base minimum rung (top-level clip, driver.cpp:442-462) */
+	int max_rung;     /* highest rung after the previous step (its top kick's max_rung) */
+	double a;         /* scale factor for the kicks and drifts of this step */
+	double tau;       /* time at the start of the step (0: first call of a run) */
+	double t0;        /* top-level step: rung r advances by t0 / 2^r */
+	double theta;
+	double hsoft;     /* softening support h, box units */
+	int bucket;       /* leaf capacity */
+	float eta;
+	float GM;
+	float max_dt;
+	int do_phi;
+	int nocrop;       /* disable the top-level clip */
+	double drag;
+	float sign;
+} ct_step_params;
+
+typedef struct {
+	ct_kick_return kr;         /* the top-level kick's return (max_rung = next step's max_rung) */
+	int minrung;               /* minimum rung for the next step (raised by the clip) */
+	int max_rung;
+	double particles_kicked;   /* sum over the ladder of active particles */
+	int kicks;                 /* ladder levels visited */
+	int particles_drifted_levels;
+} ct_step_return;
+
+ct_status ct_step_hierarchical(ct_ctx* ctx, int box_id, const ct_step_params* params, ct_step_return* result);
+/* Particle counts per rung 0..15 (particles_rung_counts, src/particles.cpp:583). */
+ct_status ct_rung_counts(ct_ctx* ctx, int box_id, uint64_t* counts);
+
 /* Tree export (breadth-first order) for inspection and parity checks. */
 ct_status ct_tree_download(ct_ctx* ctx, int box_id, ct_node* nodes, int64_t max_nodes, int64_t* count);
 

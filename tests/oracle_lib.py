@@ -169,3 +169,57 @@ def load(build=True):
         subprocess.check_call(["make", "-s", "-C", ORACLE_DIR, "libct_oracle.so"])
     _cached = Oracle(LIB)
     return _cached
+
+
+def step_hierarchical(O, st, sp, order=7, nthreads=0):
+    """The oracle's hierarchical step (src/driver.cpp:382-593) over particle state `st`
+    (dict with x, y, z, v, rung, rung_begin, stack) and step parameters `sp` (dict with the
+    fields of ct_step_params).  Mirrors ct_step_hierarchical; returns (top kick return,
+    minrung, max_rung)."""
+    minrung = sp["minrung"]
+    max_rung = max(sp["max_rung"], minrung)
+    levels = list(range(max_rung, minrung, -1)) + [minrung]
+    ascending, clip_top = True, False
+    x, y, z, v, r = st["x"], st["y"], st["z"], st["v"], st["rung"]
+    top_kr = None
+    li = 0
+    while li < len(levels):
+        level = levels[li]
+        top = level == minrung
+        if top:
+            ascending = False
+        if not ascending and not top:
+            st["stack"].append(st["rung_begin"])
+        if not ascending:
+            st["rung_begin"] = O.sort_by_rung(x, y, z, v, r, level, st["rung_begin"]) if level > 0 else 0
+        if top and minrung == sp["minrung0"]:
+            counts = np.bincount(np.clip(r, 0, 15), minlength=16)
+            if np.nonzero(counts)[0].max() > sp["minrung0"]:
+                fast = counts[sp["minrung0"] + 1:].sum()
+                slow = counts[sp["minrung0"]]
+                if 3 * fast > slow:
+                    clip_top = not sp["nocrop"]
+        nodes = O.tree_build(x, y, z, v, r, sp["theta"], sp["hsoft"], sp["bucket"], order=order, begin=st["rung_begin"])
+        kp = KickParams(sign=sp["sign"], min_rung=level, a=sp["a"], t0=sp["t0"], theta=sp["theta"], h=sp["hsoft"], eta=sp["eta"], GM=sp["GM"],
+                        max_dt=sp["max_dt"], save_force=0, first_call=int(sp["tau"] == 0.0), ascending=int(ascending or top),
+                        descending=int(False if (clip_top and top) else ((not ascending) or top)),
+                        top=int(True if (clip_top and level == sp["minrung0"] + 1) else top), do_phi=int(sp["do_phi"] and top))
+        _, kr, _ = O.kick(kp, nodes, x, y, z, v, r, order=order, nthreads=nthreads, save_force=False)
+        if clip_top and top:
+            np.maximum(r, sp["minrung0"] + 1, out=r)
+        if top:
+            top_kr = kr
+        if clip_top and top:
+            levels.append(sp["minrung0"] + 1)
+        elif (not ascending) or top:
+            max_rung = kr.max_rung
+            if max_rung > level:
+                levels.append(level + 1)
+        if ((not ascending) or top) and not (clip_top and top):
+            O.drift(x, y, z, v, r, level, sp["a"], (1.0 / (1 << level)) * sp["t0"], sp["drag"])
+        if ascending and not top:
+            st["rung_begin"] = st["stack"].pop()
+        li += 1
+    if clip_top:
+        minrung += 1
+    return top_kr, minrung, max_rung

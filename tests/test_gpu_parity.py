@@ -225,3 +225,40 @@ def test_ensemble_matches_separate_boxes(ctx):
         assert abs(krs[s].kin - kr.kin) <= 1e-9 * abs(kr.kin)
         b.close()
     ens.close()
+
+
+def test_hierarchical_steps_match_oracle(ctx, oracle):
+    """Three multistep steps (the rung ladder of kick_step_hierarchical) on the device and in
+    the oracle from the same clustered start: same ladder, rungs, positions and velocities."""
+    import cosmictiger_b200 as ct
+    from tests import oracle_lib
+
+    x, y, z, v, r = ics.clustered_box(16, nspheres=20, seed=31)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    sp = dict(minrung=0, minrung0=0, max_rung=0, a=1.0, tau=0.0, t0=0.02, theta=0.55, hsoft=h, bucket=128, eta=ics.eta_default(),
+              GM=1.0 / N, max_dt=1e30, do_phi=1, nocrop=1, drag=0.0, sign=1.0)
+    box = ctx.box(N)
+    box.upload(x, y, z, v, r)
+    st = {"x": x.copy(), "y": y.copy(), "z": z.copy(), "v": v.copy(), "rung": r.copy(), "rung_begin": 0, "stack": []}
+    gmax, omax = 0, 0
+    for step in range(3):
+        p = ct.StepParams(**sp)
+        p.max_rung = gmax
+        p.tau = step * sp["t0"]
+        res = box.step_hierarchical(p)
+        sp2 = dict(sp)
+        sp2["max_rung"] = omax
+        sp2["tau"] = step * sp["t0"]
+        okr, omin, omax = oracle_lib.step_hierarchical(oracle, st, sp2)
+        gmax = res.max_rung
+        assert res.max_rung == omax, (step, res.max_rung, omax)
+    out = box.download()
+    same_x = np.mean((out["x"] == st["x"]) & (out["y"] == st["y"]) & (out["z"] == st["z"]))
+    same_r = np.mean(out["rung"] == st["rung"])
+    verr = rel_rms(out["v"].astype(np.float64), st["v"].astype(np.float64))
+    print("hierarchical: max rung %d, identical positions %.5f, identical rungs %.5f, velocity rel rms %.3g" % (gmax, same_x, same_r, verr))
+    assert gmax >= 2
+    assert same_r > 0.999 and same_x > 0.99
+    assert verr < 1e-4
+    box.close()
