@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--n", type=int, default=256, help="particles = n^3")
     ap.add_argument("--theta", type=float, default=0.55)
     ap.add_argument("--workload", default="clustered", choices=["clustered", "lattice"])
+    ap.add_argument("--mode", default="multistep", choices=["multistep", "single"],
+                    help="multistep: hierarchical rung ladder (kick_step_hierarchical); single: all particles every step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--accuracy-sinks", type=int, default=0, help="FP64 direct-Ewald check on this many sinks (0: skip)")
@@ -148,8 +150,9 @@ def make_ics(args, seed):
 
 
 def workload_name(args):
+    steps = "4-rung hierarchical steps" if args.mode == "multistep" else "all particles per step"
     if args.workload == "clustered":
-        return "clustered %d^3 (70%% Zel'dovich k^-1.5 / 30%% Plummer), theta %.2f, order 7, Ewald, all particles per step" % (args.n, args.theta)
+        return "clustered %d^3 (70%% Zel'dovich k^-1.5 / 30%% Plummer), theta %.2f, order 7, Ewald, %s" % (args.n, args.theta, steps)
     return "lattice %d^3 Zel'dovich k^-2, theta %.2f, order 7, Ewald, all particles per step" % (args.n, args.theta)
 
 
@@ -243,9 +246,34 @@ def main():
         box.drift(0, 1.0, t0)
         return kr
 
-    # warm-up (the first is the reference's first call: no ascending half kick)
-    for i in range(args.warmup):
-        step(i == 0)
+    ms = None
+    if args.mode == "multistep":
+        # choose t0 so that the rung rule dt = eta sqrt(a h / |g|) (kick.cu:133-136) spreads the
+        # particles over rungs 0-3: 1% of them want rung >= 3
+        box.tree_create(theta, h, 128)
+        box.kick(ct.KickParams.make(theta=theta, h=h, GM=GM, eta=eta, t0=1.0, save_force=True, descending=False, ascending=False))
+        g = box.download(forces=True)
+        gm = np.sqrt(g["gx"].astype(np.float64) ** 2 + g["gy"] ** 2 + g["gz"] ** 2)
+        dts = eta * np.sqrt(h / np.maximum(gm, 1e-30))
+        ms = {"t0": float(8.0 * np.percentile(dts, 1))}
+        box.upload(x, y, z, v, r)
+        box.sort_by_rung(0)
+        ms["state"] = dict(minrung=0, max_rung=0, tau=0.0)
+
+        def mstep():
+            s = ms["state"]
+            sp = ct.StepParams(minrung=s["minrung"], minrung0=0, max_rung=s["max_rung"], a=1.0, tau=s["tau"], t0=ms["t0"], theta=theta, hsoft=h,
+                               bucket=128, eta=eta, GM=GM, max_dt=1e30, do_phi=1, nocrop=0, drag=0.0, sign=1.0)
+            res = box.step_hierarchical(sp)
+            s["minrung"], s["max_rung"], s["tau"] = res.minrung, res.max_rung, s["tau"] + ms["t0"]
+            return res
+
+        for i in range(args.warmup):
+            mstep()
+    else:
+        # warm-up (the first is the reference's first call: no ascending half kick)
+        for i in range(args.warmup):
+            step(i == 0)
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
@@ -266,8 +294,14 @@ def main():
     leaf_ms = []
     walk_ms, m2l_ms, tree_ms = [], [], []
     counters = None
+    kicked = 0.0
     for i in range(args.steps):
-        step(False)
+        if ms is not None:
+            res = mstep()
+            kicked += res.particles_kicked
+        else:
+            step(False)
+            kicked += N
         c = box.counters()
         leaf_ms.append(c["ms_leaf"])
         walk_ms.append(c["ms_walk"])
@@ -288,21 +322,37 @@ def main():
         pg.all_reduce(tt, op=pg.ReduceOp.MAX)
         t_max = float(tt.item())
     value = N * world * args.steps / (t_max / 1e3)
+    multistep = None
+    if ms is not None:
+        rc = box.rung_counts()
+        multistep = {"t0": ms["t0"], "rung_counts": [int(q) for q in rc[:8]], "active_kicks_per_step": kicked / args.steps,
+                     "active_kicks_s": kicked * world / (t_max / 1e3), "minrung": ms["state"]["minrung"], "max_rung": ms["state"]["max_rung"]}
+
     # ---- e2e through the public API with host buffers
     e2e = None
     if not args.no_e2e:
-        hx, hy, hz = (torch.from_numpy(a.copy()).pin_memory().numpy() for a in (x, y, z))
-        hv = torch.from_numpy(v.copy()).pin_memory().numpy()
-        hr = torch.from_numpy(r.copy()).pin_memory().numpy()
+        cur = box.download()
+        hx, hy, hz = (torch.from_numpy(cur[k].view(np.int32).copy()).pin_memory().numpy().view(np.uint32) for k in ("x", "y", "z"))
+        hv = torch.from_numpy(cur["v"].copy()).pin_memory().numpy()
+        hr = torch.from_numpy(cur["rung"].copy()).pin_memory().numpy()
         ox, oy, oz = (torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32) for _ in range(3))
         ov = torch.empty((N, 3), dtype=torch.float32).pin_memory().numpy()
         orr = torch.empty(N, dtype=torch.int8).pin_memory().numpy()
 
         def e2e_step(first):
             box.upload(hx, hy, hz, hv, hr)
-            step(first)
+            if ms is not None:
+                mstep()
+            else:
+                step(first)
             p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
             ctx.check(ctx.lib.ct_box_download(ctx.h, box.id, p(ox), p(oy), p(oz), p(ov), p(orr), None, None, None, None), "download")
+            # the next step starts from this step's result
+            np.copyto(hx, ox)
+            np.copyto(hy, oy)
+            np.copyto(hz, oz)
+            np.copyto(hv, ov)
+            np.copyto(hr, orr)
 
         e2e_step(True)
         torch.cuda.synchronize()
@@ -323,6 +373,31 @@ def main():
             ms_e = float(tt.item())
         e2e = {"value": N * world * ke / (ms_e / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(N * (12 + 12 + 1)),
                "d2h_bytes_per_step": int(N * (12 + 12 + 1))}
+    if multistep is not None:
+        # the all-particles step on the same box, for reference and for the leaf roofline
+        box.upload(x, y, z, v, r)
+        box.sort_by_rung(0)
+        for i in range(2):
+            step(i == 0)
+        ctx.synchronize()
+        e0s = torch.cuda.Event(enable_timing=True)
+        e1s = torch.cuda.Event(enable_timing=True)
+        e0s.record(lib_stream)
+        ks = max(2, min(args.steps, 3))
+        leaf_ms, walk_ms, m2l_ms, tree_ms = [], [], [], []
+        for i in range(ks):
+            step(False)
+            c = box.counters()
+            leaf_ms.append(c["ms_leaf"])
+            walk_ms.append(c["ms_walk"])
+            m2l_ms.append(c["ms_m2l"])
+            tree_ms.append(c["ms_tree"])
+            counters = c
+        e1s.record(lib_stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        multistep["single_rung_particle_steps_s"] = N * ks / (e0s.elapsed_time(e1s) / 1e3)
+        multistep["single_rung_ms_per_step"] = e0s.elapsed_time(e1s) / ks
     # ---- roofline of the leaf kernel (reference flop convention)
     L = ctx.lib
     L.ct_fp32_peak.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
@@ -380,6 +455,8 @@ def main():
             line["force_error"] = acc
         if ens_res:
             line["ensemble"] = ens_res
+        if multistep:
+            line["multistep"] = multistep
         print(json.dumps(line), flush=True)
     box.close()
     ctx.close()

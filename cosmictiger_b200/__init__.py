@@ -153,6 +153,11 @@ def library():
     L.ct_box_count.argtypes = [vp, i32]
     L.ct_ensemble_set_params.argtypes = [vp, i32, vp, vp]
     L.ct_kick_ensemble.argtypes = [vp, i32, ctypes.POINTER(KickParams), ctypes.POINTER(KickReturn)]
+    L.ct_ensemble_set_first_call.argtypes = [vp, i32, vp]
+    L.ct_ensemble_gather.argtypes = [vp, i32, ctypes.POINTER(i32), i32]
+    L.ct_ensemble_scatter.argtypes = [vp, i32, ctypes.POINTER(i32), i32]
+    L.ct_bytes_in_use.argtypes = [vp]
+    L.ct_bytes_in_use.restype = ctypes.c_size_t
     L.ct_step_hierarchical.argtypes = [vp, i32, ctypes.POINTER(StepParams), ctypes.POINTER(StepReturn)]
     L.ct_rung_counts.argtypes = [vp, i32, vp]
     L.ct_launch_count.argtypes = [vp]
@@ -188,6 +193,9 @@ class Context:
     def ensemble(self, counts):
         """Independent periodic boxes handled together (ct_ensemble_create)."""
         return Box(self, int(np.sum(counts)), counts=counts)
+
+    def bytes_in_use(self):
+        return int(self.lib.ct_bytes_in_use(self.h))
 
     def launches(self):
         """Kernels of libct_gravity launched on this context so far."""
@@ -234,6 +242,20 @@ class Box:
         h = np.ascontiguousarray(h, np.float32)
         GM = np.ascontiguousarray(GM, np.float32)
         self.ctx.check(self.ctx.lib.ct_ensemble_set_params(self.ctx.h, self.id, _p(h), _p(GM)), "ct_ensemble_set_params")
+
+    def set_first_call(self, flags):
+        f = np.ascontiguousarray(flags, np.int32)
+        self.ctx.check(self.ctx.lib.ct_ensemble_set_first_call(self.ctx.h, self.id, _p(f)), "ct_ensemble_set_first_call")
+
+    def gather(self, boxes):
+        """Copy plain boxes (device-resident) into this ensemble's slots."""
+        ids = (ctypes.c_int * len(boxes))(*[b.id for b in boxes])
+        self.ctx.check(self.ctx.lib.ct_ensemble_gather(self.ctx.h, self.id, ids, len(boxes)), "ct_ensemble_gather")
+
+    def scatter(self, boxes):
+        """Copy this ensemble's slots back into plain boxes."""
+        ids = (ctypes.c_int * len(boxes))(*[b.id for b in boxes])
+        self.ctx.check(self.ctx.lib.ct_ensemble_scatter(self.ctx.h, self.id, ids, len(boxes)), "ct_ensemble_scatter")
 
     def kick_ensemble(self, params):
         """Per-box kick returns of an ensemble."""

@@ -383,6 +383,7 @@ ct_status sort_by_rung_run(Ctx* c, Box* b, int minrung) {
 	cudaStream_t st = c->stream;
 	if (minrung == 0) {
 		b->rung_begin = 0;
+		b->rung_stack.clear();
 		b->tree_valid = false;
 		return CT_OK;
 	}
@@ -670,6 +671,70 @@ ct_status ct_ensemble_set_params(ct_ctx* ctx, int box_id, const float* h, const 
 	return CT_OK;
 }
 
+// Device-to-device moves between plain boxes and the slots of an ensemble.
+static ct_status ensemble_move(Ctx* c, int ens_id, const int* boxes, int count, bool gather) {
+	Box* e = get_box(c, ens_id);
+	if (!e || !boxes || count != e->nsub) {
+		return fail(c, CT_ERR_ARG, "ensemble gather/scatter: bad arguments");
+	}
+	cudaSetDevice(c->device);
+	cudaStream_t st = c->stream;
+	for (int s = 0; s < count; s++) {
+		Box* b = get_box(c, boxes[s]);
+		const int64_t off = e->sub_off[s], n = e->sub_off[s + 1] - e->sub_off[s];
+		if (!b || b->n != n || b->nsub != 1) {
+			return fail(c, CT_ERR_ARG, "ensemble gather/scatter: box size differs from its slot");
+		}
+		for (int d = 0; d < 3; d++) {
+			if (gather) {
+				CT_CUDA(c, cudaMemcpyAsync(e->x[d] + off, b->x[d], sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+				CT_CUDA(c, cudaMemcpyAsync(e->v[d] + off, b->v[d], sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+			} else {
+				CT_CUDA(c, cudaMemcpyAsync(b->x[d], e->x[d] + off, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, st));
+				CT_CUDA(c, cudaMemcpyAsync(b->v[d], e->v[d] + off, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+			}
+		}
+		if (gather) {
+			CT_CUDA(c, cudaMemcpyAsync(e->rung + off, b->rung, n, cudaMemcpyDeviceToDevice, st));
+		} else {
+			CT_CUDA(c, cudaMemcpyAsync(b->rung, e->rung + off, n, cudaMemcpyDeviceToDevice, st));
+			b->tree_valid = false;
+			b->rung_begin = 0;
+		}
+	}
+	if (gather) {
+		e->tree_valid = false;
+		e->rung_begin = 0;
+	}
+	return CT_OK;
+}
+
+ct_status ct_ensemble_set_first_call(ct_ctx* ctx, int box_id, const int* first_call) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || !first_call) {
+		return fail(c, CT_ERR_ARG, "ct_ensemble_set_first_call: bad arguments");
+	}
+	cudaSetDevice(c->device);
+	if (!b->d_sub_first) {
+		CT_TRY(dalloc(c, (void**) &b->d_sub_first, sizeof(int) * b->nsub, "box first-call flags"));
+	}
+	CT_CUDA(c, cudaMemcpy(b->d_sub_first, first_call, sizeof(int) * b->nsub, cudaMemcpyHostToDevice));
+	return CT_OK;
+}
+
+ct_status ct_ensemble_gather(ct_ctx* ctx, int ens_id, const int* boxes, int count) {
+	return ensemble_move((Ctx*) ctx, ens_id, boxes, count, true);
+}
+
+ct_status ct_ensemble_scatter(ct_ctx* ctx, int ens_id, const int* boxes, int count) {
+	return ensemble_move((Ctx*) ctx, ens_id, boxes, count, false);
+}
+
+size_t ct_bytes_in_use(const ct_ctx* ctx) {
+	return ctx ? ((const Ctx*) ctx)->used : 0;
+}
+
 int ct_box_count(const ct_ctx* ctx, int box_id) {
 	Box* b = get_box((Ctx*) ctx, box_id);
 	return b ? b->nsub : -1;
@@ -704,6 +769,7 @@ ct_status ct_box_destroy(ct_ctx* ctx, int box_id) {
 	dfree(c, b->d_sub_maxrung, sizeof(int) * b->nsub);
 	dfree(c, b->d_sub_h, sizeof(float) * b->nsub);
 	dfree(c, b->d_sub_GM, sizeof(float) * b->nsub);
+	dfree(c, b->d_sub_first, sizeof(int) * b->nsub);
 	delete b;
 	c->boxes[box_id] = nullptr;
 	return CT_OK;
@@ -736,8 +802,9 @@ static ct_status upload_impl(Ctx* c, Box* b, const uint32_t* x, const uint32_t* 
 		CT_CUDA(c, cudaMemcpyAsync(b->rung, rung, n, kind, st));
 	}
 	CT_CUDA(c, cudaGetLastError());
+	// particle data are replaced in place; the active range of the last ct_sort_by_rung (and
+	// the hierarchical step's range stack) is kept
 	b->tree_valid = false;
-	b->rung_begin = 0;
 	return CT_OK;
 }
 

@@ -108,6 +108,7 @@ struct Box {
 	float* d_sub_h = nullptr;      // per-box softening (null: the kick's h for all)
 	float* d_sub_GM = nullptr;     // per-box GM (null: the kick's GM for all)
 	std::vector<float> sub_h_host;
+	int* d_sub_first = nullptr;    // per-box first_call flag (null: the kick's flag for all)
 	std::vector<int64_t> rung_stack;  // saved active-range starts (particles_push_rungs)
 	// kick results
 	ct_counters counters;

@@ -839,6 +839,7 @@ struct P2PArgs {
 	const int64_t* sub_off;
 	const float* sub_h;
 	const NodeW* nodes;
+	const int32_t* nbox;  // tight boxes of the nodes
 	const int2* items;  // (leaf node, tile)
 	int64_t nitems;
 	const int2* pp;
@@ -881,7 +882,77 @@ __device__ __forceinline__ void pair_kernel(float r2, float h2, float hinv, floa
 	}
 }
 
-__global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
+// Smallest distance between two leaves' tight boxes (fixed<int,29> raw, 6 per node) under the
+// periodic wrap, squared, in box units.
+__device__ __forceinline__ float box_gap2(const int32_t* a, const int32_t* b) {
+	float g2 = 0.f;
+#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		// centre distance (wrapped to the nearest image) minus the two half widths
+		const int64_t ca = (int64_t) a[d] + a[3 + d], cb = (int64_t) b[d] + b[3 + d];  // 2 x centre
+		int64_t dc = ca - cb;                                                          // 2^30 = one box
+		if (dc > ((int64_t) 1 << 29)) {
+			dc -= (int64_t) 1 << 30;
+		} else if (dc < -((int64_t) 1 << 29)) {
+			dc += (int64_t) 1 << 30;
+		}
+		const int64_t adc = dc < 0 ? -dc : dc;
+		const int64_t w = ((int64_t) a[3 + d] - a[d]) + ((int64_t) b[3 + d] - b[d]);
+		const int64_t gap = adc - w;  // 2 x gap, 2^-30 units
+		if (gap > 0) {
+			const float gf = (float) gap * (1.0f / 1073741824.0f);
+			g2 += gf * gf;
+		}
+	}
+	return g2;
+}
+
+// Sum over staged sources [0, cnt) for one sink.  CHECK: pairs may fall inside the softening
+// length (per-pair test); otherwise every pair is known to be farther than h.
+template<bool CHECK>
+__device__ __forceinline__ void p2p_chunk(const float4* __restrict__ my, int cnt, float kx, float ky, float kz, float h2, float hinv, float h2inv,
+		float h3inv, float& fx, float& fy, float& fz, float& pt) {
+	float gx = 0.f, gy = 0.f, gz = 0.f, qt = 0.f;
+	int j = 0;
+	if (!CHECK) {
+#pragma unroll 4
+		for (; j + 1 < cnt; j += 2) {
+			const float4 s0 = my[j];
+			const float4 s1 = my[j + 1];
+			const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
+			const float dx1 = kx - s1.x, dy1 = ky - s1.y, dz1 = kz - s1.z;
+			const float r1a = rsqrt_ftz(fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0)));
+			const float r1b = rsqrt_ftz(fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1)));
+			const float r3a = r1a * r1a * r1a;
+			const float r3b = r1b * r1b * r1b;
+			fx = fmaf(dx0, r3a, fx);
+			fy = fmaf(dy0, r3a, fy);
+			fz = fmaf(dz0, r3a, fz);
+			pt -= r1a;
+			gx = fmaf(dx1, r3b, gx);
+			gy = fmaf(dy1, r3b, gy);
+			gz = fmaf(dz1, r3b, gz);
+			qt -= r1b;
+		}
+	}
+	for (; j < cnt; j++) {
+		const float4 s0 = my[j];
+		const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
+		const float r20 = fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0));
+		float r1a, r3a;
+		pair_kernel(r20, h2, hinv, h2inv, h3inv, r1a, r3a);
+		fx = fmaf(dx0, r3a, fx);
+		fy = fmaf(dy0, r3a, fy);
+		fz = fmaf(dz0, r3a, fz);
+		pt -= r1a;
+	}
+	fx += gx;
+	fy += gy;
+	fz += gz;
+	pt += qt;
+}
+
+__global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 	__shared__ float4 stage[P2P_TPB / 32][P2P_STAGE];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -893,6 +964,9 @@ __global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
 		const NodeW self = a.nodes[item.x];
 		const float h = a.sub_h ? a.sub_h[box_of(a.sub_off, a.nsub, self.pbeg)] : a.h;
 		const float h2 = h * h, hinv = 1.f / h, h2inv = hinv * hinv, h3inv = h2inv * hinv;
+		// a source leaf needs the per-pair softening test only if its box comes within h of the
+		// sink leaf's box (margin far above the boxes' truncation and float rounding)
+		const float near2 = h2 * 1.01f;
 		const int k = self.pbeg + 32 * item.y + lane;
 		const bool active = k < self.pend;
 		float kx = 0.f, ky = 0.f, kz = 0.f;
@@ -904,74 +978,47 @@ __global__ void __launch_bounds__(P2P_TPB) k_p2p(P2PArgs a) {
 		float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, cp = 0.f;
 		const int2 ppl = a.pp[item.x];
 		int64_t np = 0;
-		for (int q = 0; q < ppl.y; q++) {
-			const NodeW src = a.nodes[a.pp_list[ppl.x + q]];
-			for (int c0 = src.pbeg; c0 < src.pend; c0 += P2P_STAGE) {
-				const int cnt = min(P2P_STAGE, src.pend - c0);
-				for (int j = lane; j < cnt; j += 32) {
-					const int pi = c0 + j;
-					my[j] = make_float4(fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z), 0.f);
-				}
-				__syncwarp();
-				// two sources per iteration with separate accumulators; the softened kernel runs
-				// only when some lane of the warp has a pair inside h (warp-uniform branch)
-				float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
-				float gx = 0.f, gy = 0.f, gz = 0.f, qt = 0.f;
-				int j = 0;
-				for (; j + 1 < cnt; j += 2) {
-					const float4 s0 = my[j];
-					const float4 s1 = my[j + 1];
-					const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
-					const float dx1 = kx - s1.x, dy1 = ky - s1.y, dz1 = kz - s1.z;
-					const float r20 = fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0));
-					const float r21 = fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1));
-					float r1a, r3a, r1b, r3b;
-					if (__any_sync(0xffffffffu, fminf(r20, r21) <= h2)) {
-						pair_kernel(r20, h2, hinv, h2inv, h3inv, r1a, r3a);
-						pair_kernel(r21, h2, hinv, h2inv, h3inv, r1b, r3b);
-					} else {
-						r1a = rsqrt_ftz(r20);
-						r3a = r1a * r1a * r1a;
-						r1b = rsqrt_ftz(r21);
-						r3b = r1b * r1b * r1b;
+		for (int qb = 0; qb < ppl.y; qb += 32) {
+			// lanes classify 32 source leaves at a time
+			int myl = 0;
+			bool near = false;
+			if (qb + lane < ppl.y) {
+				myl = a.pp_list[ppl.x + qb + lane];
+				near = box_gap2(a.nbox + 6 * (int64_t) item.x, a.nbox + 6 * (int64_t) myl) <= near2;
+			}
+			const unsigned nmask = __ballot_sync(0xffffffffu, near);
+			const int qn = min(32, ppl.y - qb);
+			for (int q = 0; q < qn; q++) {
+				const int sl = __shfl_sync(0xffffffffu, myl, q);
+				const NodeW src = a.nodes[sl];
+				const bool check = (nmask >> q) & 1u;
+				for (int c0 = src.pbeg; c0 < src.pend; c0 += P2P_STAGE) {
+					const int cnt = min(P2P_STAGE, src.pend - c0);
+					for (int j = lane; j < cnt; j += 32) {
+						const int pi = c0 + j;
+						my[j] = make_float4(fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z), 0.f);
 					}
-					fx = fmaf(dx0, r3a, fx);
-					fy = fmaf(dy0, r3a, fy);
-					fz = fmaf(dz0, r3a, fz);
-					pt -= r1a;
-					gx = fmaf(dx1, r3b, gx);
-					gy = fmaf(dy1, r3b, gy);
-					gz = fmaf(dz1, r3b, gz);
-					qt -= r1b;
+					__syncwarp();
+					float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
+					if (check) {
+						p2p_chunk<true>(my, cnt, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+					} else {
+						p2p_chunk<false>(my, cnt, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+					}
+					__syncwarp();
+					if (a.compensated) {
+						ksum(sx, cx, fx);
+						ksum(sy, cy, fy);
+						ksum(sz, cz, fz);
+						ksum(sp, cp, pt);
+					} else {
+						sx += fx;
+						sy += fy;
+						sz += fz;
+						sp += pt;
+					}
+					np += cnt;
 				}
-				if (j < cnt) {
-					const float4 s0 = my[j];
-					const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
-					const float r20 = fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0));
-					float r1a, r3a;
-					pair_kernel(r20, h2, hinv, h2inv, h3inv, r1a, r3a);
-					fx = fmaf(dx0, r3a, fx);
-					fy = fmaf(dy0, r3a, fy);
-					fz = fmaf(dz0, r3a, fz);
-					pt -= r1a;
-				}
-				fx += gx;
-				fy += gy;
-				fz += gz;
-				pt += qt;
-				__syncwarp();
-				if (a.compensated) {
-					ksum(sx, cx, fx);
-					ksum(sy, cy, fy);
-					ksum(sz, cz, fz);
-					ksum(sp, cp, pt);
-				} else {
-					sx += fx;
-					sy += fy;
-					sz += fz;
-					sp += pt;
-				}
-				np += cnt;
 			}
 		}
 		if (active) {
@@ -994,6 +1041,7 @@ struct KickTileArgs {
 	int* sub_maxrung;
 	const float* sub_h;
 	const float* sub_GM;
+	const int* sub_first;
 	const NodeW* nodes;
 	const float* multi;
 	const float* Lx;
@@ -1034,6 +1082,7 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 		const int bx = a.nsub > 1 ? box_of(a.sub_off, a.nsub, self.pbeg) : 0;
 		const float hh = a.sub_h ? a.sub_h[bx] : kp.h;
 		const float GM = a.sub_GM ? a.sub_GM[bx] : kp.GM;
+		const bool first_call = a.sub_first ? a.sub_first[bx] != 0 : kp.first_call != 0;
 		const float hinv = 1.f / hh;
 		const int k = self.pbeg + 32 * item.y + lane;
 		const bool active = k < self.pend;
@@ -1092,7 +1141,7 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 			const float rdt = 1.0f / (float) (1 << kp.min_rung);
 			if (kp.ascending) {
 				const float dt = 0.5f * rdt * kp.t0;
-				if (!kp.first_call) {
+				if (!first_call) {
 					vx = fmaf(sgn * Fx, dt, vx);
 					vy = fmaf(sgn * Fy, dt, vy);
 					vz = fmaf(sgn * Fz, dt, vz);
@@ -1417,6 +1466,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			pa.sub_off = b->d_sub_off;
 			pa.sub_h = b->d_sub_h;
 			pa.nodes = b->nodes;
+			pa.nbox = b->nbox;
 			pa.items = items;
 			pa.nitems = nitems;
 			pa.pp = o.pp;
@@ -1439,6 +1489,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			ka.sub_maxrung = b->d_sub_maxrung;
 			ka.sub_h = b->d_sub_h;
 			ka.sub_GM = b->d_sub_GM;
+			ka.sub_first = b->d_sub_first;
 			if (b->nsub > 1) {
 				CT_CUDA(c, cudaMemsetAsync(b->d_sub_sums, 0, sizeof(double) * 9 * b->nsub, st));
 				CT_CUDA(c, cudaMemsetAsync(b->d_sub_maxrung, 0, sizeof(int) * b->nsub, st));

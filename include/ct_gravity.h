@@ -128,6 +128,15 @@ ct_status ct_ensemble_create(ct_ctx* ctx, int nbox, const int64_t* counts, int* 
 /* Per-box softening h and GM of an ensemble (box s: h[s], GM[s]); without this call every box
  * uses the kick's h and GM.  The tree build's leaf criterion uses the tree parameters' hsoft. */
 ct_status ct_ensemble_set_params(ct_ctx* ctx, int box_id, const float* h, const float* GM);
+/* Per-box first_call flags of an ensemble (boxes joining a batch start their own runs). */
+ct_status ct_ensemble_set_first_call(ct_ctx* ctx, int box_id, const int* first_call);
+/* Copy the particles of plain boxes boxes[0..count) into the ensemble's slots (gather) or
+ * back (scatter), device to device; count must equal the ensemble's box count and box s must
+ * have the size of slot s. */
+ct_status ct_ensemble_gather(ct_ctx* ctx, int ens_id, const int* boxes, int count);
+ct_status ct_ensemble_scatter(ct_ctx* ctx, int ens_id, const int* boxes, int count);
+/* Device bytes currently allocated by the context (compared against its HBM budget). */
+size_t ct_bytes_in_use(const ct_ctx* ctx);
 /* Number of boxes of an ensemble (1 for a plain box). */
 int ct_box_count(const ct_ctx* ctx, int box_id);
 /* Kick of every box of an ensemble; results[s] receives box s's kick_return. */
@@ -136,7 +145,8 @@ ct_status ct_kick_ensemble(ct_ctx* ctx, int box_id, const ct_kick_params* params
 /* Host <-> device transfers.  x,y,z: fixed32 positions (uint32, 2^-32 box units);
  * vxyz: float[3*n] interleaved velocities (the reference's particles_v layout);
  * rung: int8[n].  Download arguments may be NULL to skip a field; g/pot only exist after a
- * kick with save_force. */
+ * kick with save_force.  An upload replaces particle data in place and keeps the active range
+ * set by ct_sort_by_rung (min_rung 0 resets it). */
 ct_status ct_box_upload(ct_ctx* ctx, int box_id, const uint32_t* x, const uint32_t* y, const uint32_t* z, const float* vxyz, const int8_t* rung);
 ct_status ct_box_download(ct_ctx* ctx, int box_id, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy,
 		float* gz, float* pot);

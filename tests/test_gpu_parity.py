@@ -254,11 +254,18 @@ def test_hierarchical_steps_match_oracle(ctx, oracle):
         gmax = res.max_rung
         assert res.max_rung == omax, (step, res.max_rung, omax)
     out = box.download()
-    same_x = np.mean((out["x"] == st["x"]) & (out["y"] == st["y"]) & (out["z"] == st["z"]))
+    # positions: the drifts integrate velocities that agree to float rounding, so compare the
+    # periodic position difference (fixed32, wrapped) with the displacement over the run
+    def wrapped(a, b):
+        return (a.astype(np.uint32) - b.astype(np.uint32)).view(np.int32).astype(np.float64)
+    dpos = np.concatenate([wrapped(out[c], st[c]) for c in "xyz"])
+    disp = np.concatenate([wrapped(out[c], x0) for c, x0 in zip("xyz", (x, y, z))])
+    perr = np.sqrt(np.mean(dpos ** 2) / np.mean(disp ** 2))
     same_r = np.mean(out["rung"] == st["rung"])
     verr = rel_rms(out["v"].astype(np.float64), st["v"].astype(np.float64))
-    print("hierarchical: max rung %d, identical positions %.5f, identical rungs %.5f, velocity rel rms %.3g" % (gmax, same_x, same_r, verr))
+    print("hierarchical: max rung %d, position rel rms %.3g, identical rungs %.5f, velocity rel rms %.3g" % (gmax, perr, same_r, verr))
     assert gmax >= 2
-    assert same_r > 0.999 and same_x > 0.99
+    assert same_r > 0.999
+    assert perr < 1e-4
     assert verr < 1e-4
     box.close()

@@ -1,0 +1,88 @@
+"""Host logic of the continuous-batching server, on a fake device context: every request
+receives exactly its number of steps, its first step is flagged as the run's first call, and
+admission keeps the resident particles within the memory budget."""
+from cosmictiger_b200 import serving
+
+
+class FakeBox:
+    def __init__(self, n):
+        self.n = n
+        self.steps = 0
+        self.closed = False
+
+    def upload(self, *state):
+        self.steps = 0
+
+    def download(self):
+        return {"steps": self.steps}
+
+    def close(self):
+        self.closed = True
+
+
+class FakeEnsemble:
+    def __init__(self, counts, log):
+        self.slots = [0] * len(counts)
+        self.first = None
+        self.log = log
+
+    def set_box_params(self, h, gm):
+        pass
+
+    def gather(self, boxes):
+        assert not any(b.closed for b in boxes)
+        self.slots = [b.steps for b in boxes]
+
+    def scatter(self, boxes):
+        assert len(boxes) == len(self.slots)
+        for b, s in zip(boxes, self.slots):
+            b.steps = s
+
+    def set_first_call(self, flags):
+        self.first = list(flags)
+
+    def tree_create(self, *args):
+        pass
+
+    def kick(self, params):
+        for s, f in zip(self.slots, self.first):
+            self.log.append((s == 0) == bool(f))
+
+    def drift(self, *args):
+        self.slots = [s + 1 for s in self.slots]
+
+    def close(self):
+        pass
+
+
+class FakeContext:
+    def __init__(self):
+        self.log = []
+        self.resident = 0
+        self.peak = 0
+
+    def box(self, n):
+        return FakeBox(n)
+
+    def ensemble(self, counts):
+        self.peak = max(self.peak, sum(counts))
+        return FakeEnsemble(counts, self.log)
+
+    def synchronize(self):
+        pass
+
+
+def test_server_steps_and_budget():
+    reqs = serving.poisson_requests(40, rate=5000.0, nmin=8, nmax=20, smin=1, smax=9, seed=11)
+    states = {r.rid: () for r in reqs}
+    budget = 3.0 * max(r.particles for r in reqs) * serving.BYTES_PER_PARTICLE
+    ctx = FakeContext()
+    srv = serving.Server(ctx, hbm_budget=budget)
+    done = srv.run(reqs, states)
+    assert sorted(r.rid for r in done) == list(range(len(reqs)))
+    for r in done:
+        assert r.result["steps"] == r.steps, (r.rid, r.result, r.steps)
+        assert r.done >= r.admitted >= r.arrival - 1e-9
+    assert all(ctx.log) and len(ctx.log) == sum(r.steps for r in reqs)
+    assert ctx.peak * serving.BYTES_PER_PARTICLE <= budget
+    assert srv.ticks < sum(r.steps for r in reqs)
