@@ -4,14 +4,18 @@
 Workload (default): the clustered 256^3 box -- 70% of 16.8M particles on a Zel'dovich-displaced
 lattice (P(k) ~ k^-1.5, 0.5 mean-spacing RMS), 30% in 20,000 Plummer spheres with power-law
 masses -- at theta = 0.55, expansion order 7, softening 1/50 of the mean spacing, Ewald on.
-A step is one tree build over all particles, one kick (forces, velocities, rungs) and one
-drift.  Inputs are seeded synthetic stand-ins generated here (no dataset is involved).
+A step (--mode multistep, the default) is one hierarchical step of kick_step_hierarchical:
+the rung ladder of sorts, tree builds over the active particles, kicks and drifts, so that
+value counts particle-steps of the whole box per device second.  --mode single kicks every
+particle each step (one tree build, one kick, one drift).  Inputs are seeded synthetic
+stand-ins generated here (no dataset is involved).
 
   value   particle-steps/s with particles resident in HBM (device-timed, CUDA events)
   e2e     the same through the public API with host buffers: every step uploads the
           particles from pinned host memory and downloads positions, velocities and rungs
-  roofline  the leaf kernel (P2P + M2P + L2P + kick, the dominant kernel) against the measured
-          FP32 FMA peak, flops counted with the reference's per-interaction convention
+  roofline  k_p2p (the particle-particle kernel, the largest share of the step) on the
+          all-particles step against the measured FP32 FMA peak, 21 flops per pair (the
+          reference's per-interaction count), timed by CUDA events on the library's stream
   cpu_baseline  the CPU oracle (this project's restatement of the reference's algorithm; the
           reference's own CPU kick cannot run) on a bounded sample of the same workload
 
@@ -291,7 +295,7 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(lib_stream)
-    leaf_ms = []
+    leaf_ms, leafkick_ms = [], []
     walk_ms, m2l_ms, tree_ms = [], [], []
     counters = None
     kicked = 0.0
@@ -304,6 +308,7 @@ def main():
             kicked += N
         c = box.counters()
         leaf_ms.append(c["ms_leaf"])
+        leafkick_ms.append(c["ms_leafkick"])
         walk_ms.append(c["ms_walk"])
         m2l_ms.append(c["ms_m2l"])
         tree_ms.append(c["ms_tree"])
@@ -384,11 +389,12 @@ def main():
         e1s = torch.cuda.Event(enable_timing=True)
         e0s.record(lib_stream)
         ks = max(2, min(args.steps, 3))
-        leaf_ms, walk_ms, m2l_ms, tree_ms = [], [], [], []
+        leaf_ms, leafkick_ms, walk_ms, m2l_ms, tree_ms = [], [], [], [], []
         for i in range(ks):
             step(False)
             c = box.counters()
             leaf_ms.append(c["ms_leaf"])
+            leafkick_ms.append(c["ms_leafkick"])
             walk_ms.append(c["ms_walk"])
             m2l_ms.append(c["ms_m2l"])
             tree_ms.append(c["ms_tree"])
@@ -405,15 +411,17 @@ def main():
     ctx.check(L.ct_fp32_peak(ctx.h, ctypes.byref(pk)), "ct_fp32_peak")
     peak_tf = pk.value
     c = counters
-    npart = N
-    leaf_flops = 21.0 * c["pp_pairs"] + c["pc_pairs"] * (6 + 265 + 520 + 119 + 4) + npart * (557 + 178)
-    leaf_s = float(np.mean(leaf_ms)) / 1e3
-    achieved = leaf_flops / leaf_s / 1e12
+    # k_p2p: 21 flops per particle pair (the reference's count, gravity.hpp), per launch
+    p2p_flops = 21.0 * c["pp_pairs"]
+    p2p_s = float(np.mean(leaf_ms)) / 1e3
+    achieved = p2p_flops / p2p_s / 1e12
     traffic = read_traffic()
-    roofline = {"bound": "fp32_fma", "kernel": "k_leaf (P2P+M2P+L2P+kick)", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
-                "frac": achieved / peak_tf if peak_tf else None, "traffic": traffic,
-                "peak_source": "measured on this GPU by ct_fp32_peak (FMA chain, 2 flops per FMA); MEASURED_PEAKS.json has no FP32 entry"}
-    extra = {"ms_tree": float(np.mean(tree_ms)), "ms_walk": float(np.mean(walk_ms)), "ms_m2l": float(np.mean(m2l_ms)), "ms_leaf": float(np.mean(leaf_ms)),
+    roofline = {"bound": "fp32_fma", "kernel": "k_p2p (particle-particle forces, all-particles step)", "achieved": achieved, "peak": peak_tf,
+                "unit": "TFLOP/s", "frac": achieved / peak_tf if peak_tf else None, "traffic": traffic,
+                "flops_per_launch": p2p_flops, "ms_per_launch": p2p_s * 1e3,
+                "peak_source": "measured on this GPU by ct_fp32_peak (FFMA chains, 2 flops per FMA); the measured peaks file has no FP32 entry"}
+    extra = {"ms_tree": float(np.mean(tree_ms)), "ms_walk": float(np.mean(walk_ms)), "ms_m2l": float(np.mean(m2l_ms)), "ms_p2p": float(np.mean(leaf_ms)),
+             "ms_leafkick": float(np.mean(leafkick_ms)),
              "pp_pairs": c["pp_pairs"], "cc_direct": c["cc_direct"], "cc_ewald": c["cc_ewald"], "pc_pairs": c["pc_pairs"], "cp_pairs": c["cp_pairs"],
              "nodes": c["nodes"], "leaves": c["leaves"], "flops_per_step": c["flops"], "wall_s": wall}
     ens_res = None
@@ -465,8 +473,8 @@ def main():
 
 
 def read_traffic():
-    """DRAM bytes per launch of the leaf kernel from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", "k_leaf_traffic.txt")
+    """DRAM bytes per launch of k_p2p from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "k_p2p_clustered192.txt")
     if not os.path.exists(p):
         return None
     try:

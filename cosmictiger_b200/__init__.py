@@ -93,7 +93,7 @@ class StepReturn(ctypes.Structure):
 class Counters(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "pp_pairs", "cc_direct", "cc_ewald", "cp_pairs", "pc_pairs", "nodes", "leaves", "flops", "flops_pp", "flops_cc",
-        "ms_tree", "ms_walk", "ms_m2l", "ms_l2l", "ms_leaf", "ms_drift", "ms_leafkick")]
+        "ms_tree", "ms_walk", "ms_m2l", "ms_l2l", "ms_leaf", "ms_drift", "ms_leafkick", "pp_near")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

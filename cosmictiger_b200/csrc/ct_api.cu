@@ -374,6 +374,7 @@ ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag) {
 				drag != 0.0);
 	}
 	cudaEventRecord(c->ev[7], c->stream);
+	c->drift_timed = true;
 	CT_CUDA(c, cudaGetLastError());
 	b->tree_valid = false;
 	return CT_OK;
@@ -915,9 +916,7 @@ ct_status ct_tree_create(ct_ctx* ctx, int box_id, const ct_tree_params* params, 
 	CT_TRY(tree_build(c, b, params));
 	cudaEventRecord(c->ev[9], c->stream);
 	cudaEventSynchronize(c->ev[9]);
-	float ms = 0.f;
-	cudaEventElapsedTime(&ms, c->ev[8], c->ev[9]);
-	b->counters.ms_tree = ms;
+	b->counters.ms_tree = elapsed_ms(c->ev[8], c->ev[9]);
 	if (node_count) {
 		*node_count = b->nnodes;
 	}
@@ -1050,9 +1049,8 @@ ct_status ct_get_counters(ct_ctx* ctx, int box_id, ct_counters* out) {
 	if (!b || !out) {
 		return fail(c, CT_ERR_ARG, "ct_get_counters: bad arguments");
 	}
-	float ms = 0.f;
-	if (cudaEventQuery(c->ev[7]) == cudaSuccess && cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]) == cudaSuccess) {
-		b->counters.ms_drift = ms;
+	if (c->drift_timed && cudaEventQuery(c->ev[7]) == cudaSuccess) {
+		b->counters.ms_drift = elapsed_ms(c->ev[6], c->ev[7]);
 	}
 	*out = b->counters;
 	return CT_OK;
@@ -1084,8 +1082,7 @@ ct_status ct_fp32_peak(ct_ctx* ctx, double* tflops) {
 		k_fma_peak<<<blocks, 256, 0, c->stream>>>(out, iters, 0.9999999f, 1e-7f);
 		cudaEventRecord(c->ev[11], c->stream);
 		CT_CUDA(c, cudaEventSynchronize(c->ev[11]));
-		float ms = 0.f;
-		cudaEventElapsedTime(&ms, c->ev[10], c->ev[11]);
+		const float ms = elapsed_ms(c->ev[10], c->ev[11]);
 		const double fl = 2.0 * 16.0 * iters * 256.0 * blocks;
 		if (rep > 0) {
 			best = std::max(best, fl / (ms * 1e-3) / 1e12);

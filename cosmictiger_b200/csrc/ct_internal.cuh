@@ -135,8 +135,21 @@ struct Ctx {
 	double* d_counters = nullptr; // interaction counters
 	void* d_ewald_tab = nullptr;  // device copy of the Ewald tables (when not in __constant__)
 	cudaEvent_t ev[16];
+	bool drift_timed = false;         // ev[6], ev[7] hold a recorded drift
 	unsigned long long launches = 0;  // kernels of this library launched so far
 };
+
+// Device time between two recorded events, 0 if it is not available.  A failed query sets the
+// runtime's last error; that error is this call's own and is cleared, so that it cannot
+// surface in a later, unrelated check (a library routine that peeks at the last error).
+inline float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
+	float ms = 0.f;
+	if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+		cudaGetLastError();
+		ms = 0.f;
+	}
+	return ms;
+}
 
 // Allocation with budget accounting.
 ct_status dalloc(Ctx* c, void** p, size_t bytes, const char* what);

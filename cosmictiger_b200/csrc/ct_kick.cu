@@ -849,6 +849,7 @@ struct P2PArgs {
 	float h;
 	int compensated;
 	double* pairs;
+	double* near_pairs;
 };
 
 // Approximate reciprocal square root (the MUFU unit), flushing denormals: pair separations
@@ -907,58 +908,124 @@ __device__ __forceinline__ float box_gap2(const int32_t* a, const int32_t* b) {
 	return g2;
 }
 
+// Packed pairs of floats for the sm_100 f32x2 instructions: one instruction applies the same
+// IEEE round-to-nearest operation to both halves, so each half is bit-identical to the scalar
+// operation while the instruction issues once.
+struct f2 {
+	uint64_t v;
+};
+__device__ __forceinline__ f2 f2_pack(float lo, float hi) {
+	f2 r;
+	asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+	return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 a, float& lo, float& hi) {
+	asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
+	f2 r;
+	asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+	return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+	f2 r;
+	asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+	return r;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+	f2 r;
+	asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+	return r;
+}
+
+// Staged sources of one warp: positions relative to the sink leaf's centre, x and y of source
+// pairs interleaved (x_2i, x_2i+1, y_2i, y_2i+1) and z by quads, so that a pair of sources
+// arrives as aligned register pairs for the f32x2 instructions.
+struct P2PStage {
+	float4 xy[P2P_STAGE / 2];
+	float4 z[P2P_STAGE / 4];
+};
+
+__device__ __forceinline__ void stage_put(P2PStage* st, int j, float x, float y, float z) {
+	float* xy = reinterpret_cast<float*>(st->xy);
+	xy[4 * (j >> 1) + (j & 1)] = x;
+	xy[4 * (j >> 1) + 2 + (j & 1)] = y;
+	reinterpret_cast<float*>(st->z)[j] = z;
+}
+
+// One staged source against one sink with the per-pair softening test.
+__device__ __forceinline__ void p2p_checked(const P2PStage* st, int j, float kx, float ky, float kz, float h2, float hinv, float h2inv, float h3inv,
+		float& fx, float& fy, float& fz, float& pt) {
+	const float* xy = reinterpret_cast<const float*>(st->xy);
+	const float dx = kx - xy[4 * (j >> 1) + (j & 1)];
+	const float dy = ky - xy[4 * (j >> 1) + 2 + (j & 1)];
+	const float dz = kz - reinterpret_cast<const float*>(st->z)[j];
+	const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+	float r1, r3;
+	pair_kernel(r2, h2, hinv, h2inv, h3inv, r1, r3);
+	fx = fmaf(dx, r3, fx);
+	fy = fmaf(dy, r3, fy);
+	fz = fmaf(dz, r3, fz);
+	pt -= r1;
+}
+
 // Sum over staged sources [0, cnt) for one sink.  CHECK: pairs may fall inside the softening
-// length (per-pair test); otherwise every pair is known to be farther than h.
+// length (per-pair test); otherwise every pair is known to be farther than h and sources go
+// two at a time through f32x2 (even sources in the low half, odd in the high half).
 template<bool CHECK>
-__device__ __forceinline__ void p2p_chunk(const float4* __restrict__ my, int cnt, float kx, float ky, float kz, float h2, float hinv, float h2inv,
+__device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int cnt, float kx, float ky, float kz, float h2, float hinv, float h2inv,
 		float h3inv, float& fx, float& fy, float& fz, float& pt) {
-	float gx = 0.f, gy = 0.f, gz = 0.f, qt = 0.f;
 	int j = 0;
 	if (!CHECK) {
-#pragma unroll 4
-		for (; j + 1 < cnt; j += 2) {
-			const float4 s0 = my[j];
-			const float4 s1 = my[j + 1];
-			const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
-			const float dx1 = kx - s1.x, dy1 = ky - s1.y, dz1 = kz - s1.z;
-			const float r1a = rsqrt_ftz(fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0)));
-			const float r1b = rsqrt_ftz(fmaf(dx1, dx1, fmaf(dy1, dy1, dz1 * dz1)));
-			const float r3a = r1a * r1a * r1a;
-			const float r3b = r1b * r1b * r1b;
-			fx = fmaf(dx0, r3a, fx);
-			fy = fmaf(dy0, r3a, fy);
-			fz = fmaf(dz0, r3a, fz);
-			pt -= r1a;
-			gx = fmaf(dx1, r3b, gx);
-			gy = fmaf(dy1, r3b, gy);
-			gz = fmaf(dz1, r3b, gz);
-			qt -= r1b;
+		const f2 KX = f2_pack(kx, kx), KY = f2_pack(ky, ky), KZ = f2_pack(kz, kz);
+		f2 ax = f2_pack(0.f, 0.f), ay = ax, az = ax, ap = ax;
+#pragma unroll 2
+		for (; j + 3 < cnt; j += 4) {
+			const float4 xy0 = st->xy[j >> 1];
+			const float4 xy1 = st->xy[(j >> 1) + 1];
+			const float4 zz = st->z[j >> 2];
+			const f2 dx0 = f2_sub(KX, f2_pack(xy0.x, xy0.y)), dy0 = f2_sub(KY, f2_pack(xy0.z, xy0.w)), dz0 = f2_sub(KZ, f2_pack(zz.x, zz.y));
+			const f2 dx1 = f2_sub(KX, f2_pack(xy1.x, xy1.y)), dy1 = f2_sub(KY, f2_pack(xy1.z, xy1.w)), dz1 = f2_sub(KZ, f2_pack(zz.z, zz.w));
+			const f2 q0 = f2_fma(dx0, dx0, f2_fma(dy0, dy0, f2_mul(dz0, dz0)));
+			const f2 q1 = f2_fma(dx1, dx1, f2_fma(dy1, dy1, f2_mul(dz1, dz1)));
+			float a0, b0, a1, b1;
+			f2_unpack(q0, a0, b0);
+			f2_unpack(q1, a1, b1);
+			const f2 r10 = f2_pack(rsqrt_ftz(a0), rsqrt_ftz(b0));
+			const f2 r11 = f2_pack(rsqrt_ftz(a1), rsqrt_ftz(b1));
+			const f2 r30 = f2_mul(f2_mul(r10, r10), r10);
+			const f2 r31 = f2_mul(f2_mul(r11, r11), r11);
+			ax = f2_fma(dx0, r30, ax);
+			ay = f2_fma(dy0, r30, ay);
+			az = f2_fma(dz0, r30, az);
+			ap = f2_sub(ap, r10);
+			ax = f2_fma(dx1, r31, ax);
+			ay = f2_fma(dy1, r31, ay);
+			az = f2_fma(dz1, r31, az);
+			ap = f2_sub(ap, r11);
 		}
+		float lo, hi;
+		f2_unpack(ax, lo, hi);
+		fx += lo + hi;
+		f2_unpack(ay, lo, hi);
+		fy += lo + hi;
+		f2_unpack(az, lo, hi);
+		fz += lo + hi;
+		f2_unpack(ap, lo, hi);
+		pt += lo + hi;
 	}
 	for (; j < cnt; j++) {
-		const float4 s0 = my[j];
-		const float dx0 = kx - s0.x, dy0 = ky - s0.y, dz0 = kz - s0.z;
-		const float r20 = fmaf(dx0, dx0, fmaf(dy0, dy0, dz0 * dz0));
-		float r1a, r3a;
-		pair_kernel(r20, h2, hinv, h2inv, h3inv, r1a, r3a);
-		fx = fmaf(dx0, r3a, fx);
-		fy = fmaf(dy0, r3a, fy);
-		fz = fmaf(dz0, r3a, fz);
-		pt -= r1a;
+		p2p_checked(st, j, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 	}
-	fx += gx;
-	fy += gy;
-	fz += gz;
-	pt += qt;
 }
 
 __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
-	__shared__ float4 stage[P2P_TPB / 32][P2P_STAGE];
+	__shared__ P2PStage stage[P2P_TPB / 32];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
-	float4* my = stage[w];
-	double npairs = 0.0;
+	P2PStage* my = &stage[w];
+	double npairs = 0.0, nnear = 0.0;
 	for (int64_t it = gw; it < a.nitems; it += nw) {
 		const int2 item = a.items[it];
 		const NodeW self = a.nodes[item.x];
@@ -977,7 +1044,7 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 		}
 		float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, cp = 0.f;
 		const int2 ppl = a.pp[item.x];
-		int64_t np = 0;
+		int64_t np = 0, nn = 0;
 		for (int qb = 0; qb < ppl.y; qb += 32) {
 			// lanes classify 32 source leaves at a time
 			int myl = 0;
@@ -996,7 +1063,7 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 					const int cnt = min(P2P_STAGE, src.pend - c0);
 					for (int j = lane; j < cnt; j += 32) {
 						const int pi = c0 + j;
-						my[j] = make_float4(fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z), 0.f);
+						stage_put(my, j, fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z));
 					}
 					__syncwarp();
 					float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
@@ -1018,19 +1085,23 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 						sp += pt;
 					}
 					np += cnt;
+					nn += check ? cnt : 0;
 				}
 			}
 		}
 		if (active) {
 			a.F[k] = make_float4(sx + cx, sy + cy, sz + cz, sp + cp);
 			npairs += (double) np;
+			nnear += (double) nn;
 		}
 	}
 	for (int o = 16; o; o >>= 1) {
 		npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
+		nnear += __shfl_xor_sync(0xffffffffu, nnear, o);
 	}
 	if (lane == 0 && npairs > 0) {
 		atomicAdd(a.pairs, npairs);
+		atomicAdd(a.near_pairs, nnear);
 	}
 }
 
@@ -1478,6 +1549,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			pa.h = kp->h;
 			pa.compensated = 1;
 			pa.pairs = counters + 4 + 7;
+			pa.near_pairs = counters + 13;
 			cudaEventRecord(c->ev[4], st);
 			c->launches++;
 			k_p2p<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
@@ -1540,6 +1612,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		C.cc_direct = (double) hcur[1];
 		C.pc_pairs = hd[12];
 		C.pp_pairs = hd[11];
+		C.pp_near = hd[13];
 		C.cp_pairs = hd[1];
 		C.nodes = (double) nn;
 		C.leaves = (double) nleaves;
@@ -1552,18 +1625,12 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 				C.cc_ewald * (3 + 7 + 140 * 92 + 540 + FLOP_M2L + phi * FLOP_M2L_PHI) + 843.0 * icnt;
 		C.flops = C.flops_pp + C.flops_cc + C.cp_pairs * (Ops::NEXP + 6 + FLOP_GREENS) + C.pc_pairs * (6 + FLOP_GREENS + FLOP_M2L2 + phi * FLOP_M2L_PHI + 4)
 				+ (double) nn * (FLOP_L2L + phi * FLOP_L2L_PHI) + (double) np * (FLOP_KICK + phi * FLOP_KICK_PHI);
-		float ms = 0;
-		cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
-		C.ms_walk = ms;
-		cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
-		C.ms_m2l = ms;
-		cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
-		C.ms_l2l = ms;
-		cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
-		C.ms_leaf = ms;  // the P2P kernel (or the fused leaf kernel)
+		C.ms_walk = elapsed_ms(c->ev[0], c->ev[1]);
+		C.ms_m2l = elapsed_ms(c->ev[1], c->ev[2]);
+		C.ms_l2l = elapsed_ms(c->ev[2], c->ev[3]);
+		C.ms_leaf = elapsed_ms(c->ev[4], c->ev[5]);  // the P2P kernel (or the fused leaf kernel)
 		if (!fused && nleaves > 0) {
-			cudaEventElapsedTime(&ms, c->ev[5], c->ev[12]);
-			C.ms_leafkick = ms;
+			C.ms_leafkick = elapsed_ms(c->ev[5], c->ev[12]);
 		}
 		b->have_force = kp->save_force != 0;
 		return CT_OK;

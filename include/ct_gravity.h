@@ -105,6 +105,8 @@ typedef struct {
 	double flops_cc;
 	double ms_tree, ms_walk, ms_m2l, ms_l2l, ms_leaf, ms_drift; /* device time of the last calls */
 	double ms_leafkick;   /* M2P + L2P + kick after the P2P kernel */
+	double pp_near;       /* pairs from source leaves within the softening length of the sink
+	                         leaf (the per-pair softening test runs on these only) */
 } ct_counters;
 
 /* ---- context */

@@ -46,6 +46,25 @@ def rel_rms(a, b):
     return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
 
 
+def test_counters_before_any_drift_leave_no_stale_error():
+    """Reading the counters before a context has drifted anything must leave no CUDA error
+    behind for the next call (the tree build's library scans check the runtime's last error)."""
+    import cosmictiger_b200 as ct
+
+    c = ct.Context(order=7)
+    x, y, z, v, r = lattice(16, seed=7)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    b = c.box(N)
+    b.upload(x, y, z, v, r)
+    for i in range(3):
+        b.tree_create(0.7, h, 128)
+        b.kick(kick_params(0.7, h, N, t0=1.0 / 64, first_call=(i == 0), save_force=False))
+        assert b.counters()["ms_drift"] == 0.0
+    b.close()
+    c.close()
+
+
 def test_drift_bitexact(ctx, oracle):
     rng = np.random.default_rng(7)
     N = 50000
