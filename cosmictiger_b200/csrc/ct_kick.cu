@@ -462,25 +462,20 @@ __global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __re
 	}
 }
 
-// Direct M2L and P2L: dL += sum over the direct CC list and the CP source particles.
+// Direct M2L: dL += sum over the direct CC list.
 template<class Ops>
 __global__ void __launch_bounds__(128) k_m2l_direct(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi,
-		const int2* __restrict__ dcc, const int* __restrict__ dcc_list, const int2* __restrict__ cp, const int* __restrict__ cp_list,
-		const uint32_t* __restrict__ x0, const uint32_t* __restrict__ x1, const uint32_t* __restrict__ x2, float* __restrict__ dL, int do_phi,
-		double* counters) {
+		const int2* __restrict__ dcc, const int* __restrict__ dcc_list, float* __restrict__ dL, int do_phi) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
-	double ncp = 0;
 	for (int64_t si = gw; si < nn; si += nw) {
 		const int2 lst = dcc[si];
-		const NodeW self = nodes[si];
-		const bool leaf = self.flags & 1;
-		const int2 cpl = leaf ? cp[si] : make_int2(0, 0);
-		if (lst.y == 0 && cpl.y == 0) {
+		if (lst.y == 0) {
 			continue;
 		}
+		const NodeW self = nodes[si];
 		float L[NE];
 		for (int i = 0; i < NE; i++) {
 			L[i] = 0.f;
@@ -501,17 +496,85 @@ __global__ void __launch_bounds__(128) k_m2l_direct(int64_t nn, const NodeW* __r
 			Ops::greens(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z));
 			Ops::m2l(L, M, D, do_phi != 0);
 		}
-		// P2L: each source particle's Green's function added to the expansion (gravity.cu:134-144)
-		for (int q = 0; q < cpl.y; q++) {
-			const NodeW src = nodes[cp_list[cpl.x + q]];
-			for (int k = src.pbeg + lane; k < src.pend; k += 32) {
-				float D[NE];
-				Ops::greens(D, fixed_dist(self.x, x0[k]), fixed_dist(self.y, x1[k]), fixed_dist(self.z, x2[k]));
-				for (int i = 0; i < NE; i++) {
-					L[i] += D[i];
+		warp_reduce_arr<NE>(L);
+		if (lane == 0) {
+			for (int i = 0; i < NE; i++) {
+				dL[NEXP_STRIDE * si + i] += L[i];
+			}
+		}
+	}
+}
+
+// P2L (gravity.cu:134-144): every particle of the leaf's CP source leaves adds its Green's
+// function to the leaf's expansion, dL += sum D(x_leaf - x_p).  The source leaves' particles
+// are taken as one flat sequence (32 leaves at a time, prefix sums of their sizes in
+// registers), so lanes stay busy across leaf boundaries; each lane prefetches its next
+// particle's position while it evaluates the current one.
+template<class Ops>
+__global__ void __launch_bounds__(128) k_p2l(int64_t nn, const NodeW* __restrict__ nodes, const int2* __restrict__ cp, const int* __restrict__ cp_list,
+		const uint32_t* __restrict__ x0, const uint32_t* __restrict__ x1, const uint32_t* __restrict__ x2, float* __restrict__ dL, double* counters) {
+	constexpr int NE = Ops::NEXP;
+	const int lane = threadIdx.x & 31;
+	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nw = (gridDim.x * blockDim.x) >> 5;
+	double ncp = 0;
+	for (int64_t si = gw; si < nn; si += nw) {
+		const int2 cpl = cp[si];
+		if (cpl.y == 0 || !(nodes[si].flags & 1)) {
+			continue;
+		}
+		const NodeW self = nodes[si];
+		float L[NE];
+		for (int i = 0; i < NE; i++) {
+			L[i] = 0.f;
+		}
+		for (int qb = 0; qb < cpl.y; qb += 32) {
+			int beg = 0, cnt = 0;
+			if (qb + lane < cpl.y) {
+				const NodeW s = nodes[cp_list[cpl.x + qb + lane]];
+				beg = s.pbeg;
+				cnt = s.pend - s.pbeg;
+			}
+			int inc = cnt;  // inclusive prefix of the sizes over lanes
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				const int t = __shfl_up_sync(0xffffffffu, inc, o);
+				inc += lane >= o ? t : 0;
+			}
+			const int total = __shfl_sync(0xffffffffu, inc, 31);
+			const int first = beg - (inc - cnt);  // particle index = first[owner] + flat index
+			ncp += total;
+			// owner lane of flat index g: the number of lanes whose inclusive prefix is <= g
+			auto particle = [&](int g) {
+				int l = 0;
+#pragma unroll
+				for (int s = 16; s; s >>= 1) {
+					l += __shfl_sync(0xffffffffu, inc, l + s - 1) <= g ? s : 0;
+				}
+				return __shfl_sync(0xffffffffu, first, l) + g;
+			};
+			int g = lane;
+			int k = particle(g);
+			uint32_t px = 0, py = 0, pz = 0;
+			if (g < total) {
+				px = x0[k];
+				py = x1[k];
+				pz = x2[k];
+			}
+			for (int gb = 0; gb < total; gb += 32) {
+				const uint32_t cx = px, cy = py, cz = pz;
+				const bool have = g < total;
+				g += 32;
+				k = particle(g);
+				if (g < total) {
+					px = x0[k];
+					py = x1[k];
+					pz = x2[k];
+				}
+				if (have) {
+					Ops::greens_add(L, fixed_dist(self.x, cx), fixed_dist(self.y, cy), fixed_dist(self.z, cz));
 				}
 			}
-			ncp += src.pend - src.pbeg;
 		}
 		warp_reduce_arr<NE>(L);
 		if (lane == 0) {
@@ -1463,8 +1526,9 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		c->launches++;
 		k_m2l_ewald<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL, kp->do_phi, counters);
 		c->launches++;
-		k_m2l_direct<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL, kp->do_phi,
-				counters);
+		k_m2l_direct<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, K.dL, kp->do_phi);
+		c->launches++;
+		k_p2l<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL, counters);
 		cudaEventRecord(c->ev[2], st);
 		for (int k = 0; k < nlev; k++) {
 			const int64_t lb = b->level_start[k], le = b->level_start[k + 1];

@@ -15,6 +15,9 @@ namespace ct {
 		template<class T> __host__ __device__ __forceinline__ static void greens(T* D, T x, T y, T z) {  \
 			NS::greens(D, x, y, z);                                                                      \
 		}                                                                                                \
+		template<class T> __host__ __device__ __forceinline__ static void greens_add(T* L, T x, T y, T z) { \
+			NS::greens_add(L, x, y, z);                                                                  \
+		}                                                                                                \
 		template<class T> __host__ __device__ __forceinline__ static int ewald(T* D, T x, T y, T z, const Tab& t) { \
 			return NS::ewald_greens(D, x, y, z, t);                                                      \
 		}                                                                                                \

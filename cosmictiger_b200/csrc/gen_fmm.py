@@ -240,7 +240,9 @@ def full_from_stored(em, arr, name, Q, needed):
     return out
 
 
-def gen_greens(P):
+def gen_greens(P, accumulate=False):
+    """D(n) = d^n(-1/r); with accumulate, L[n] += D(n) instead (the same product, then one
+    add per entry: identical roundings to computing D and adding it)."""
     em = Emitter()
     stored = tl_stored(P)
     em("x *= T(%g); y *= T(%g); z *= T(%g);" % (SCALE, SCALE, SCALE))
@@ -267,7 +269,10 @@ def gen_greens(P):
         sub_em.ind = em.ind + 1
         emit_sum(sub_em, "s", terms, None)
         em.lines.extend(sub_em.lines)
-        em("\tD[%d] = s * rp%d;" % (tl_index(n, P), N + 1))
+        if accumulate:
+            em("\tL[%d] += s * rp%d;" % (tl_index(n, P), N + 1))
+        else:
+            em("\tD[%d] = s * rp%d;" % (tl_index(n, P), N + 1))
         em("}")
     return em.text()
 
@@ -487,6 +492,11 @@ def gen_header(P):
     h.append("// D(n) = d^n(-1/r) at (x,y,z) (box units; scaled by 1e3 inside). fmm_kernels.hpp:52-307")
     h.append("template<class T> CT_HD void greens(T* __restrict__ D, T x, T y, T z) {")
     h.append(gen_greens(P).rstrip())
+    h.append("}")
+    h.append("")
+    h.append("// L(n) += D(n) at (x,y,z): P2L of a unit mass, without storing D. gravity.cu:134-144")
+    h.append("template<class T> CT_HD void greens_add(T* __restrict__ L, T x, T y, T z) {")
+    h.append(gen_greens(P, accumulate=True).rstrip())
     h.append("}")
     h.append("")
     h.append("// Add the radial-function derivative tensor: Dr[n] += sum_m n!/(2^|m| m!(n-2m)!) u^(n-2m) g_(|n|-|m|) rinv^|m|,")
