@@ -1109,31 +1109,52 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 		const int2 ppl = a.pp[item.x];
 		int64_t np = 0, nn = 0;
 		for (int qb = 0; qb < ppl.y; qb += 32) {
-			// lanes classify 32 source leaves at a time
-			int myl = 0;
+			// lanes take 32 source leaves at a time: particle range and class (near: the leaf's
+			// box comes within h of the sink leaf's box, so pairs need the softening test)
+			int beg = 0, cnt = 0;
 			bool near = false;
 			if (qb + lane < ppl.y) {
-				myl = a.pp_list[ppl.x + qb + lane];
-				near = box_gap2(a.nbox + 6 * (int64_t) item.x, a.nbox + 6 * (int64_t) myl) <= near2;
+				const int sl = a.pp_list[ppl.x + qb + lane];
+				const int2 pr = *reinterpret_cast<const int2*>(&a.nodes[sl].pbeg);
+				beg = pr.x;
+				cnt = pr.y - pr.x;
+				near = box_gap2(a.nbox + 6 * (int64_t) item.x, a.nbox + 6 * (int64_t) sl) <= near2;
 			}
-			const unsigned nmask = __ballot_sync(0xffffffffu, near);
-			const int qn = min(32, ppl.y - qb);
-			for (int q = 0; q < qn; q++) {
-				const int sl = __shfl_sync(0xffffffffu, myl, q);
-				const NodeW src = a.nodes[sl];
-				const bool check = (nmask >> q) & 1u;
-				for (int c0 = src.pbeg; c0 < src.pend; c0 += P2P_STAGE) {
-					const int cnt = min(P2P_STAGE, src.pend - c0);
-					for (int j = lane; j < cnt; j += 32) {
-						const int pi = c0 + j;
-						stage_put(my, j, fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z));
+			// far leaves first, then near ones; the particles of one class form a single flat
+			// sequence (prefix sums of the leaf sizes over lanes), staged P2P_STAGE at a time
+			for (int cls = 0; cls < 2; cls++) {
+				const bool check = cls != 0;
+				const int c = near == check ? cnt : 0;
+				int inc = c;
+#pragma unroll
+				for (int o = 1; o < 32; o <<= 1) {
+					const int t = __shfl_up_sync(0xffffffffu, inc, o);
+					inc += lane >= o ? t : 0;
+				}
+				const int total = __shfl_sync(0xffffffffu, inc, 31);
+				const int first = beg - (inc - c);  // particle index = first[owner] + flat index
+				for (int gb = 0; gb < total; gb += P2P_STAGE) {
+					const int n = min(P2P_STAGE, total - gb);
+#pragma unroll
+					for (int j = lane; j < P2P_STAGE; j += 32) {
+						const int g = gb + j;
+						// owner lane of flat index g: the lanes whose inclusive prefix is <= g
+						int l = 0;
+#pragma unroll
+						for (int st = 16; st; st >>= 1) {
+							l += __shfl_sync(0xffffffffu, inc, l + st - 1) <= g ? st : 0;
+						}
+						const int pi = __shfl_sync(0xffffffffu, first, l) + g;
+						if (g < total) {
+							stage_put(my, j, fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z));
+						}
 					}
 					__syncwarp();
 					float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
 					if (check) {
-						p2p_chunk<true>(my, cnt, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+						p2p_chunk<true>(my, n, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 					} else {
-						p2p_chunk<false>(my, cnt, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+						p2p_chunk<false>(my, n, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 					}
 					__syncwarp();
 					if (a.compensated) {
@@ -1147,8 +1168,8 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 						sz += fz;
 						sp += pt;
 					}
-					np += cnt;
-					nn += check ? cnt : 0;
+					np += n;
+					nn += check ? n : 0;
 				}
 			}
 		}
