@@ -895,7 +895,7 @@ __global__ void __launch_bounds__(LEAF_TPB) k_leaf(LeafArgs a) {
 // P2P alone (warp per 32-sink tile of a leaf, sources staged per warp in shared memory as
 // float4 positions relative to the leaf centre), then M2P + L2P + kick per tile.
 constexpr int P2P_TPB = 256;
-constexpr int P2P_STAGE = 64;
+constexpr int P2P_STAGE = 128;
 
 struct P2PArgs {
 	int nsub;
@@ -1042,11 +1042,11 @@ __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int c
 	if (!CHECK) {
 		const f2 KX = f2_pack(kx, kx), KY = f2_pack(ky, ky), KZ = f2_pack(kz, kz);
 		f2 ax = f2_pack(0.f, 0.f), ay = ax, az = ax, ap = ax;
-#pragma unroll 2
-		for (; j + 3 < cnt; j += 4) {
-			const float4 xy0 = st->xy[j >> 1];
-			const float4 xy1 = st->xy[(j >> 1) + 1];
-			const float4 zz = st->z[j >> 2];
+		// four sources (two f32x2 pairs) starting at q, a multiple of 4
+		auto quad = [&](int q) {
+			const float4 xy0 = st->xy[q >> 1];
+			const float4 xy1 = st->xy[(q >> 1) + 1];
+			const float4 zz = st->z[q >> 2];
 			const f2 dx0 = f2_sub(KX, f2_pack(xy0.x, xy0.y)), dy0 = f2_sub(KY, f2_pack(xy0.z, xy0.w)), dz0 = f2_sub(KZ, f2_pack(zz.x, zz.y));
 			const f2 dx1 = f2_sub(KX, f2_pack(xy1.x, xy1.y)), dy1 = f2_sub(KY, f2_pack(xy1.z, xy1.w)), dz1 = f2_sub(KZ, f2_pack(zz.z, zz.w));
 			const f2 q0 = f2_fma(dx0, dx0, f2_fma(dy0, dy0, f2_mul(dz0, dz0)));
@@ -1066,6 +1066,19 @@ __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int c
 			ay = f2_fma(dy1, r31, ay);
 			az = f2_fma(dz1, r31, az);
 			ap = f2_sub(ap, r11);
+		};
+		if (cnt == P2P_STAGE) {
+			// a full chunk: constant offsets, no loop arithmetic
+#pragma unroll
+			for (int q = 0; q < P2P_STAGE; q += 4) {
+				quad(q);
+			}
+			j = P2P_STAGE;
+		} else {
+#pragma unroll 2
+			for (; j + 3 < cnt; j += 4) {
+				quad(j);
+			}
 		}
 		float lo, hi;
 		f2_unpack(ax, lo, hi);
@@ -1253,9 +1266,14 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 			const int c = a.pc_list[pcl.x + q];
 			const NodeW ot = a.nodes[c];
 			float M[NM], D[NE], L2[5] = { 0.f, 0.f, 0.f, 0.f, 0.f };
-			const float* mp = a.multi + (size_t) NMULT_STRIDE * c;
-			for (int i = 0; i < NM; i++) {
-				M[i] = __ldg(mp + i);
+			const float4* mp = (const float4*) (a.multi + (size_t) NMULT_STRIDE * c);
+#pragma unroll
+			for (int i = 0; i < (NM + 3) / 4; i++) {
+				const float4 v = __ldg(mp + i);
+				if (4 * i + 0 < NM) M[4 * i + 0] = v.x;
+				if (4 * i + 1 < NM) M[4 * i + 1] = v.y;
+				if (4 * i + 2 < NM) M[4 * i + 2] = v.z;
+				if (4 * i + 3 < NM) M[4 * i + 3] = v.w;
 			}
 			Ops::greens(D, fixed_dist(X[0], ot.x), fixed_dist(X[1], ot.y), fixed_dist(X[2], ot.z));
 			Ops::m2l2(L2, M, D, kp.do_phi != 0);

@@ -241,8 +241,8 @@ def full_from_stored(em, arr, name, Q, needed):
 
 
 def gen_greens(P, accumulate=False):
-    """D(n) = d^n(-1/r); with accumulate, L[n] += D(n) instead (the same product, then one
-    add per entry: identical roundings to computing D and adding it)."""
+    """D(n) = d^n(-1/r); with accumulate, L[n] += D(n) instead, the final scaling by
+    r^-(|n|+1) fused with the add (one FMA per entry)."""
     em = Emitter()
     stored = tl_stored(P)
     em("x *= T(%g); y *= T(%g); z *= T(%g);" % (SCALE, SCALE, SCALE))
@@ -270,7 +270,7 @@ def gen_greens(P, accumulate=False):
         emit_sum(sub_em, "s", terms, None)
         em.lines.extend(sub_em.lines)
         if accumulate:
-            em("\tL[%d] += s * rp%d;" % (tl_index(n, P), N + 1))
+            em("\tL[%d] = ct_fma(s, rp%d, L[%d]);" % (tl_index(n, P), N + 1, tl_index(n, P)))
         else:
             em("\tD[%d] = s * rp%d;" % (tl_index(n, P), N + 1))
         em("}")
@@ -494,7 +494,8 @@ def gen_header(P):
     h.append(gen_greens(P).rstrip())
     h.append("}")
     h.append("")
-    h.append("// L(n) += D(n) at (x,y,z): P2L of a unit mass, without storing D. gravity.cu:134-144")
+    h.append("// L(n) += D(n) at (x,y,z): P2L of a unit mass, without storing D (each entry's")
+    h.append("// r^-(|n|+1) scaling fused with the add). gravity.cu:134-144")
     h.append("template<class T> CT_HD void greens_add(T* __restrict__ L, T x, T y, T z) {")
     h.append(gen_greens(P, accumulate=True).rstrip())
     h.append("}")

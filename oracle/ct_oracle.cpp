@@ -98,6 +98,9 @@ struct Ops7 {
 	template<class T> static void greens(T* D, T x, T y, T z) {
 		ct_p7::greens(D, x, y, z);
 	}
+	template<class T> static void greens_add(T* L, T x, T y, T z) {
+		ct_p7::greens_add(L, x, y, z);
+	}
 	static int ewald(float* D, float x, float y, float z) {
 		return ct_p7::ewald_greens(D, x, y, z, tab());
 	}
@@ -133,6 +136,9 @@ struct Ops5 {
 	static constexpr int NEXP = ct_p5::NEXP, NMULT = ct_p5::NMULT;
 	template<class T> static void greens(T* D, T x, T y, T z) {
 		ct_p5::greens(D, x, y, z);
+	}
+	template<class T> static void greens_add(T* L, T x, T y, T z) {
+		ct_p5::greens_add(L, x, y, z);
 	}
 	static int ewald(float* D, float x, float y, float z) {
 		return ct_p5::ewald_greens(D, x, y, z, tab());
@@ -699,14 +705,11 @@ void walk(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const uint3
 				for (int c : cp) {
 					const ct_or_node& o = nodes[c];
 					for (int j = o.part_begin; j < o.part_end; j++) {
-						float dx[3], D[Ops::NEXP];
+						float dx[3];
 						for (int d = 0; d < 3; d++) {
 							dx[d] = fdist(self.pos[d], C.x[d][j]);
 						}
-						Ops::greens(D, dx[0], dx[1], dx[2]);
-						for (int k = 0; k < Ops::NEXP; k++) {
-							Lacc[k] += D[k];
-						}
+						Ops::greens_add(Lacc, dx[0], dx[1], dx[2]);
 						acc.flops += Ops::NEXP + 6 + FLOP_GREENS;
 					}
 				}
