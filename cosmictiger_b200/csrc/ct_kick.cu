@@ -1252,17 +1252,17 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 		const float GM = a.sub_GM ? a.sub_GM[bx] : kp.GM;
 		const bool first_call = a.sub_first ? a.sub_first[bx] != 0 : kp.first_call != 0;
 		const float hinv = 1.f / hh;
-		const int k = self.pbeg + 32 * item.y + lane;
-		const bool active = k < self.pend;
-		uint32_t X[3] = { self.x, self.y, self.z };
-		if (active) {
-			X[0] = a.x[0][k];
-			X[1] = a.x[1][k];
-			X[2] = a.x[2][k];
-		}
-		float Fx = 0.f, Fy = 0.f, Fz = 0.f, Fp = (693.f / 256.f) * hinv;
+		// S sinks in this tile; with at most 16, R = 32 / S lanes (replicas) share each sink's
+		// M2P list (replica r takes every R-th source node); every lane holds a real sink
+		const int S = max(1, min(32, self.pend - (self.pbeg + 32 * item.y)));
+		const int R = S <= 16 ? 32 / S : 1;
+		const int sink = lane % S, rep = lane / S;
+		const int k = self.pbeg + 32 * item.y + sink;
+		const bool active = rep == 0;
+		const uint32_t X[3] = { a.x[0][k], a.x[1][k], a.x[2][k] };
+		float Fx = 0.f, Fy = 0.f, Fz = 0.f, Fp = rep == 0 ? (693.f / 256.f) * hinv : 0.f;
 		const int2 pcl = a.pc[item.x];
-		for (int q = 0; q < pcl.y; q++) {
+		for (int q = rep < R ? rep : 0; q < pcl.y; q += R) {
 			const int c = a.pc_list[pcl.x + q];
 			const NodeW ot = a.nodes[c];
 			float M[NM], D[NE], L2[5] = { 0.f, 0.f, 0.f, 0.f, 0.f };
@@ -1281,6 +1281,17 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 			Fy -= 1e6f * L2[2];
 			Fz -= 1e6f * L2[3];
 			Fp += 1e3f * L2[0];
+		}
+		if (R > 1) {
+			// replica 0 adds the other replicas' sums, in replica order (lane sink + t S <= 31)
+			const float ox = Fx, oy = Fy, oz = Fz, op = Fp;
+			for (int t = 1; t < R; t++) {
+				const int src = sink + t * S;
+				Fx += __shfl_sync(0xffffffffu, ox, src);
+				Fy += __shfl_sync(0xffffffffu, oy, src);
+				Fz += __shfl_sync(0xffffffffu, oz, src);
+				Fp += __shfl_sync(0xffffffffu, op, src);
+			}
 		}
 		double ia[9];
 		for (int q = 0; q < 9; q++) {
