@@ -41,7 +41,7 @@ import numpy as np  # noqa: E402
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="particles = n^3")
@@ -51,7 +51,7 @@ def parse():
                     help="multistep: hierarchical rung ladder (kick_step_hierarchical); single: all particles every step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--accuracy-sinks", type=int, default=0, help="FP64 direct-Ewald check on this many sinks (0: skip)")
+    ap.add_argument("--accuracy-sinks", type=int, default=10000, help="FP64 direct-Ewald check on this many seeded sinks (0: skip)")
     ap.add_argument("--ensemble-boxes", type=int, default=64, help="boxes of the batched-vs-plain ensemble comparison (0: skip)")
     ap.add_argument("--ensemble-nmin", type=int, default=16)
     ap.add_argument("--ensemble-nmax", type=int, default=64)

@@ -1,0 +1,66 @@
+"""ctypes binding of oracle/_ref/libctref_gpu.so: the reference's own CUDA kick and drift
+(src/kick.cu, src/gravity.cu, src/drift.cu and the rest of its device code, compiled from the
+reference's sources for sm_100a by `make -C oracle refgpu`) behind a small host harness
+(oracle/ref_gpu_shim.cu).  Test infrastructure only.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libctref_gpu.so")
+
+
+class RefKickParams(ctypes.Structure):
+    """kick_params fields in the reference's meaning (cosmictiger/kick.hpp:138-186)."""
+    _fields_ = [("sign", ctypes.c_float), ("min_rung", ctypes.c_int), ("a", ctypes.c_float), ("t0", ctypes.c_float), ("theta", ctypes.c_float),
+                ("h", ctypes.c_float), ("eta", ctypes.c_float), ("GM", ctypes.c_float), ("max_dt", ctypes.c_float), ("save_force", ctypes.c_int),
+                ("first_call", ctypes.c_int), ("ascending", ctypes.c_int), ("descending", ctypes.c_int), ("top", ctypes.c_int), ("do_phi", ctypes.c_int)]
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def available():
+    return os.path.exists(LIB)
+
+
+class ReferenceGPU:
+    def __init__(self, heap_bytes=1 << 30):
+        L = ctypes.CDLL(LIB)
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        L.ctref_init.argtypes = [ctypes.c_double]
+        L.ctref_kick.argtypes = [i64, vp, vp, vp, vp, vp, i64, vp, ctypes.POINTER(RefKickParams), vp, vp, vp, vp, vp]
+        L.ctref_drift.argtypes = [i64, i64, vp, vp, vp, vp, vp, ctypes.c_int, ctypes.c_float, ctypes.c_float]
+        rc = L.ctref_init(float(heap_bytes))
+        if rc != 0:
+            raise RuntimeError("reference harness set-up failed (%d)" % rc)
+        self.lib = L
+
+    def kick(self, state, nodes, params):
+        """Kick every particle with the reference's kernel (whole walk from the root).
+        state: tree-ordered x, y, z (uint32), v (float32 (n,3)), rung (int8); nodes: the tree
+        as exported by Box.tree() (breadth-first, root first)."""
+        x, y, z = (np.ascontiguousarray(state[k], np.uint32) for k in "xyz")
+        v = np.ascontiguousarray(state["v"], np.float32).copy()
+        r = np.ascontiguousarray(state["rung"], np.int8).copy()
+        n = len(x)
+        g = [np.zeros(n, np.float32) for _ in range(4)]
+        ret = np.zeros(8)
+        nodes = np.ascontiguousarray(nodes)
+        rc = self.lib.ctref_kick(n, _p(x), _p(y), _p(z), _p(v), _p(r), len(nodes), _p(nodes), ctypes.byref(params), *[_p(a) for a in g], _p(ret))
+        if rc != 0:
+            raise RuntimeError("reference kick failed (%d)" % rc)
+        return {"v": v, "rung": r, "gx": g[0], "gy": g[1], "gz": g[2], "pot": g[3], "max_rung": int(ret[0]), "pot_sum": ret[1], "kin": ret[2]}
+
+    def drift(self, x, y, z, v, rung, level, a, dt, rung_begin=0):
+        """Drift (in place on copies) the particles in [rung_begin, n) of rung `level`."""
+        x, y, z = (np.ascontiguousarray(q, np.uint32).copy() for q in (x, y, z))
+        v = np.ascontiguousarray(v, np.float32)
+        rung = np.ascontiguousarray(rung, np.int8)
+        rc = self.lib.ctref_drift(len(x), rung_begin, _p(x), _p(y), _p(z), _p(v), _p(rung), level, a, dt)
+        if rc != 0:
+            raise RuntimeError("reference drift failed (%d)" % rc)
+        return x, y, z
