@@ -1035,10 +1035,13 @@ __device__ __forceinline__ void p2p_checked(const P2PStage* st, int j, float kx,
 // Sum over staged sources [0, cnt) for one sink.  CHECK: pairs may fall inside the softening
 // length (per-pair test); otherwise every pair is known to be farther than h and sources go
 // two at a time through f32x2 (even sources in the low half, odd in the high half).
+//
+// Sources [jb, je) of the chunk (jb a multiple of 4): the whole chunk for a full tile, a slice
+// for one replica of a small tile.
 template<bool CHECK>
-__device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int cnt, float kx, float ky, float kz, float h2, float hinv, float h2inv,
-		float h3inv, float& fx, float& fy, float& fz, float& pt) {
-	int j = 0;
+__device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int jb, int je, float kx, float ky, float kz, float h2, float hinv,
+		float h2inv, float h3inv, float& fx, float& fy, float& fz, float& pt) {
+	int j = jb;
 	if (!CHECK) {
 		const f2 KX = f2_pack(kx, kx), KY = f2_pack(ky, ky), KZ = f2_pack(kz, kz);
 		f2 ax = f2_pack(0.f, 0.f), ay = ax, az = ax, ap = ax;
@@ -1067,7 +1070,7 @@ __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int c
 			az = f2_fma(dz1, r31, az);
 			ap = f2_sub(ap, r11);
 		};
-		if (cnt == P2P_STAGE) {
+		if (jb == 0 && je == P2P_STAGE) {
 			// a full chunk: constant offsets, no loop arithmetic
 #pragma unroll
 			for (int q = 0; q < P2P_STAGE; q += 4) {
@@ -1076,7 +1079,7 @@ __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int c
 			j = P2P_STAGE;
 		} else {
 #pragma unroll 2
-			for (; j + 3 < cnt; j += 4) {
+			for (; j + 3 < je; j += 4) {
 				quad(j);
 			}
 		}
@@ -1090,11 +1093,15 @@ __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int c
 		f2_unpack(ap, lo, hi);
 		pt += lo + hi;
 	}
-	for (; j < cnt; j++) {
+	for (; j < je; j++) {
 		p2p_checked(st, j, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 	}
 }
 
+// SMALL: tiles of at most 16 sinks.  S' = S rounded up to a power of two lanes hold the sinks
+// (lanes past S repeat a sink and are not written); the 32 / S' groups of S' lanes (replicas)
+// each take a contiguous slice of every staged chunk and are added by a butterfly at the end.
+template<bool SMALL>
 __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 	__shared__ P2PStage stage[P2P_TPB / 32];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1110,10 +1117,18 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 		// a source leaf needs the per-pair softening test only if its box comes within h of the
 		// sink leaf's box (margin far above the boxes' truncation and float rounding)
 		const float near2 = h2 * 1.01f;
-		const int k = self.pbeg + 32 * item.y + lane;
-		const bool active = k < self.pend;
+		int sl = lane, rep = 0, Sp = 32;
+		if (SMALL) {
+			const int S = max(1, self.pend - (self.pbeg + 32 * item.y));  // 1..16
+			Sp = S <= 1 ? 1 : 1 << (32 - __clz(S - 1));
+			sl = lane & (Sp - 1);
+			rep = lane / Sp;
+			sl = sl < S ? sl : sl - S;  // sl < Sp < 2S
+		}
+		const int k = self.pbeg + 32 * item.y + sl;
+		const bool active = SMALL ? (rep == 0 && (lane & (Sp - 1)) == sl) : k < self.pend;
 		float kx = 0.f, ky = 0.f, kz = 0.f;
-		if (active) {
+		if (SMALL || active) {
 			kx = fixed_dist(a.x[0][k], self.x);
 			ky = fixed_dist(a.x[1][k], self.y);
 			kz = fixed_dist(a.x[2][k], self.z);
@@ -1164,10 +1179,17 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 					}
 					__syncwarp();
 					float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
+					int jb = 0, je = n;
+					if (SMALL) {
+						const int R = 32 / Sp;
+						const int sub = ((n + R - 1) / R + 3) & ~3;
+						jb = min(n, rep * sub);
+						je = min(n, jb + sub);
+					}
 					if (check) {
-						p2p_chunk<true>(my, n, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+						p2p_chunk<true>(my, jb, je, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 					} else {
-						p2p_chunk<false>(my, n, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+						p2p_chunk<false>(my, jb, je, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 					}
 					__syncwarp();
 					if (a.compensated) {
@@ -1186,8 +1208,17 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 				}
 			}
 		}
+		float tx = sx + cx, ty = sy + cy, tz = sz + cz, tp = sp + cp;
+		if (SMALL) {
+			for (int o = Sp; o < 32; o <<= 1) {
+				tx += __shfl_xor_sync(0xffffffffu, tx, o);
+				ty += __shfl_xor_sync(0xffffffffu, ty, o);
+				tz += __shfl_xor_sync(0xffffffffu, tz, o);
+				tp += __shfl_xor_sync(0xffffffffu, tp, o);
+			}
+		}
 		if (active) {
-			a.F[k] = make_float4(sx + cx, sy + cy, sz + cz, sp + cp);
+			a.F[k] = make_float4(tx, ty, tz, tp);
 			npairs += (double) np;
 			nnear += (double) nn;
 		}
@@ -1199,6 +1230,22 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 	if (lane == 0 && npairs > 0) {
 		atomicAdd(a.pairs, npairs);
 		atomicAdd(a.near_pairs, nnear);
+	}
+}
+
+// Tiles with more than 16 sinks to `big`, the others to `small` (order within each list is
+// immaterial: every tile computes its own sinks).
+__global__ void k_split_tiles(const int2* __restrict__ items, int64_t nitems, const NodeW* __restrict__ nodes, int2* big, int2* small,
+		unsigned long long* counts) {
+	for (int64_t it = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; it < nitems; it += (int64_t) gridDim.x * blockDim.x) {
+		const int2 item = items[it];
+		const NodeW nd = nodes[item.x];
+		const int S = nd.pend - (nd.pbeg + 32 * item.y);
+		if (S > 16) {
+			big[atomicAdd(counts, 1ull)] = item;
+		} else {
+			small[atomicAdd(counts + 1, 1ull)] = item;
+		}
 	}
 }
 
@@ -1664,9 +1711,30 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			pa.compensated = 1;
 			pa.pairs = counters + 4 + 7;
 			pa.near_pairs = counters + 13;
-			cudaEventRecord(c->ev[4], st);
+			// full tiles and tiles of at most 16 sinks go to separate launches
+			int2* tiles2 = (int2*) scratch(c, 45, sizeof(int2) * 2 * (nitems + 1), &s2);
+			CT_TRY(s2);
+			unsigned long long* tcount = (unsigned long long*) (c->d_flags + 44);
+			CT_CUDA(c, cudaMemsetAsync(tcount, 0, 2 * sizeof(unsigned long long), st));
 			c->launches++;
-			k_p2p<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
+			k_split_tiles<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 255) / 256, c->nsm * 8)), 256, 0, st>>>(items, nitems, b->nodes, tiles2,
+					tiles2 + nitems + 1, tcount);
+			CT_CUDA(c, cudaMemcpyAsync(hf, tcount, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+			CT_CUDA(c, cudaStreamSynchronize(st));
+			const int64_t nbig = (int64_t) ((unsigned long long*) hf)[0], nsmall = (int64_t) ((unsigned long long*) hf)[1];
+			cudaEventRecord(c->ev[4], st);
+			if (nbig > 0) {
+				pa.items = tiles2;
+				pa.nitems = nbig;
+				c->launches++;
+				k_p2p<false><<<(int) std::max<int64_t>(1, std::min<int64_t>((nbig + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
+			}
+			if (nsmall > 0) {
+				pa.items = tiles2 + nitems + 1;
+				pa.nitems = nsmall;
+				c->launches++;
+				k_p2p<true><<<(int) std::max<int64_t>(1, std::min<int64_t>((nsmall + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
+			}
 			cudaEventRecord(c->ev[5], st);
 			KickTileArgs ka;
 			ka.nsub = b->nsub;
