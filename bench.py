@@ -56,6 +56,11 @@ def parse():
     ap.add_argument("--ensemble-nmin", type=int, default=16)
     ap.add_argument("--ensemble-nmax", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=3)
+    ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving"],
+                    help="instead of the benchmark line: precision (theta x order x summation, force error vs FP64 Ewald and "
+                         "particle-steps/s), ensemble (512 boxes of 16^3..128^3, batched vs box by box, 20 steps) or serving "
+                         "(Poisson arrivals of 32^3..256^3 requests, rate sweep, p50/p99 latency vs sequential runs)")
+    ap.add_argument("--study-seed", type=int, default=11)
     return ap.parse_args()
 
 
@@ -217,6 +222,10 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference(args)
+        return
+    if args.study != "none":
+        if rank == 0:
+            run_study(args)
         return
     import torch
 
@@ -572,6 +581,134 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": info["cores"], "kind": "port", "sample": info["sample"]},
             "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def force_errors(box, theta, h, N, nsink, seed):
+    """Kick every particle with save_force, then compare nsink seeded sinks with the FP64
+    direct Ewald sum (same definitions as the benchmark line's force_error)."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import ics
+
+    box.tree_create(theta, h, 128)
+    box.kick(ct.KickParams.make(theta=theta, h=h, GM=1.0 / N, eta=ics.eta_default(), save_force=True, descending=False, ascending=False))
+    out = box.download(forces=True)
+    sel = np.sort(np.random.default_rng(seed).choice(N, size=min(nsink, N), replace=False))
+    dg = box.direct_ewald(out["x"][sel], out["y"][sel], out["z"][sel], h)
+    gt = np.stack([out["gx"][sel], out["gy"][sel], out["gz"][sel]], 1).astype(np.float64)
+    gd = np.stack(dg[:3], 1) / N
+    err = np.linalg.norm(gt - gd, axis=1) / np.linalg.norm(gd, axis=1)
+    return {"rms": float(np.sqrt(np.sum((gt - gd) ** 2) / np.sum(gd ** 2))), "rms_per_particle": float(np.sqrt(np.mean(err ** 2))),
+            "p99_per_particle": float(np.percentile(err, 99))}
+
+
+def timed_steps(torch, ctx, box, theta, h, N, steps, lib_stream):
+    """Device time of `steps` all-particle steps (tree build, kick, drift) after one warm-up."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import ics
+
+    def step(first):
+        box.tree_create(theta, h, 128)
+        box.kick(ct.KickParams.make(theta=theta, h=h, GM=1.0 / N, eta=ics.eta_default(), t0=1.0 / 64, first_call=first, save_force=False))
+        box.drift(0, 1.0, 1.0 / 64)
+
+    step(True)
+    ctx.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(lib_stream)
+    for i in range(steps):
+        step(False)
+    e1.record(lib_stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def study_precision(args, torch):
+    """Precision study (the clustered generator with a varied seed): theta in {0.4, 0.55, 0.7} x
+    expansion order in {5, 7} x compensated / plain FP32 P2P sums; force error against the
+    FP64 direct Ewald sum on seeded sinks and particle-steps/s of the all-particles step."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import ics
+
+    state = make_ics(args, seed=args.study_seed)
+    N = len(state[0])
+    h = ics.softening(N, 0.02)
+    nsink = args.accuracy_sinks if args.accuracy_sinks > 0 else 1000
+    rows = []
+    for order in (5, 7):
+        ctx = ct.Context(order=order)
+        lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
+        box = ctx.box(N)
+        for theta in (0.4, 0.55, 0.7):
+            for comp in (True, False):
+                ctx.set_compensated(comp)
+                box.upload(*state)
+                ms = timed_steps(torch, ctx, box, theta, h, N, 2, lib_stream)
+                box.upload(*state)
+                err = force_errors(box, theta, h, N, nsink, seed=4321)
+                row = {"order": order, "theta": theta, "summation": "compensated" if comp else "plain", "ms_per_step": ms,
+                       "particle_steps_s": N / (ms / 1e3), **err}
+                rows.append(row)
+                print(json.dumps(row), flush=True)
+        box.close()
+        ctx.close()
+    return {"study": "precision", "workload": workload_name(args).replace("4-rung hierarchical steps", "all particles per step") + ", seed %d" % args.study_seed,
+            "particles": N, "sinks": nsink, "rows": rows}
+
+
+def study_ensemble(args, torch):
+    """512 independent boxes, n_i log-uniform in [16, 128], own Zel'dovich fields, theta 0.55,
+    20 steps: one batched ensemble vs the plain single-box path launched box by box."""
+    import cosmictiger_b200 as ct
+
+    ctx = ct.Context(order=7)
+    lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
+    a = argparse.Namespace(**vars(args))
+    a.ensemble_boxes, a.ensemble_nmin, a.ensemble_nmax, a.ensemble_steps = 512, 16, 128, 20
+    res = ensemble_compare(ct, torch, ctx, a, args.theta, lib_stream)
+    ctx.close()
+    return {"study": "ensemble", **res}
+
+
+def study_serving(args, torch):
+    """Continuous batching: open-loop Poisson arrivals of requests for boxes of n^3 particles, n
+    log-uniform in [32, 256], 1-16 steps each, admission by a 150 GB device-memory budget; a sweep
+    of arrival rates, each against the same requests served one at a time in arrival order."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import serving
+
+    ctx = ct.Context(order=7)
+    count = 24
+    states = {}
+    out = []
+    for rate in (1.0, 2.0, 4.0, 8.0):
+        reqs = serving.poisson_requests(count, rate=rate, nmin=32, nmax=256, smin=1, smax=16, seed=args.study_seed)
+        for r in reqs:
+            if r.rid not in states:
+                states[r.rid] = serving.request_state(r)
+        srv = serving.Server(ctx, theta=args.theta, hbm_budget=150e9)
+        done = srv.run(reqs, states)
+        s_b = serving.summarize(done)
+        seq = serving.poisson_requests(count, rate=rate, nmin=32, nmax=256, smin=1, smax=16, seed=args.study_seed)
+        s_p = serving.summarize(serving.run_sequential(ctx, seq, states, theta=args.theta))
+        row = {"rate_per_s": rate, "requests": count, "batched": s_b, "sequential": s_p, "ticks": srv.ticks,
+               "throughput_ratio": s_b["particle_steps_s"] / s_p["particle_steps_s"]}
+        out.append(row)
+        print(json.dumps(row), flush=True)
+    ctx.close()
+    return {"study": "serving", "n_range": [32, 256], "steps_range": [1, 16], "hbm_budget_gb": 150, "rows": out}
+
+
+def run_study(args):
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    fn = {"precision": study_precision, "ensemble": study_ensemble, "serving": study_serving}[args.study]
+    t = time.perf_counter()
+    res = fn(args, torch)
+    res["wall_s"] = time.perf_counter() - t
+    print(json.dumps(res), flush=True)
 
 
 if __name__ == "__main__":

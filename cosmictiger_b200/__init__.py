@@ -143,6 +143,7 @@ def library():
     L.ct_box_download.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ct_box_download_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ct_sort_by_rung.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
+    L.ct_ctx_set_compensated.argtypes = [vp, i32]
     L.ct_tree_create.argtypes = [vp, i32, ctypes.POINTER(TreeParams), ctypes.POINTER(i64)]
     L.ct_kick.argtypes = [vp, i32, ctypes.POINTER(KickParams), ctypes.POINTER(KickReturn)]
     L.ct_drift.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_double]
@@ -200,6 +201,10 @@ class Context:
     def launches(self):
         """Kernels of libct_gravity launched on this context so far."""
         return int(self.lib.ct_launch_count(self.h))
+
+    def set_compensated(self, on):
+        """Neumaier-compensated (True, default) or plain FP32 sums of the P2P source batches."""
+        self.check(self.lib.ct_ctx_set_compensated(self.h, int(bool(on))), "ct_ctx_set_compensated")
 
     def synchronize(self):
         self.check(self.lib.ct_synchronize(self.h), "ct_synchronize")

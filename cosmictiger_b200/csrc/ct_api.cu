@@ -1065,6 +1065,15 @@ ct_status ct_synchronize(ct_ctx* ctx) {
 	return CT_OK;
 }
 
+ct_status ct_ctx_set_compensated(ct_ctx* ctx, int compensated) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c) {
+		return CT_ERR_ARG;
+	}
+	c->compensated = compensated != 0;
+	return CT_OK;
+}
+
 ct_status ct_fp32_peak(ct_ctx* ctx, double* tflops) {
 	Ctx* c = (Ctx*) ctx;
 	if (!c || !tflops) {

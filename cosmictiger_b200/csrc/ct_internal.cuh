@@ -137,6 +137,7 @@ struct Ctx {
 	cudaEvent_t ev[16];
 	bool drift_timed = false;         // ev[6], ev[7] hold a recorded drift
 	unsigned long long launches = 0;  // kernels of this library launched so far
+	int compensated = 1;              // Neumaier-compensated P2P batch sums
 };
 
 // Device time between two recorded events, 0 if it is not available.  A failed query sets the

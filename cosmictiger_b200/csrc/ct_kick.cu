@@ -1425,6 +1425,12 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 					atomicAdd(a.sub_sums + 9 * lo + q, ia[q]);
 				}
 				atomicMax(a.sub_maxrung + lo, imax);
+			} else {
+				// every lane now holds the warp's totals: only lane 0 carries them into the
+				// context-wide sums below
+				for (int q = 0; q < 9; q++) {
+					ia[q] = 0.0;
+				}
 			}
 		}
 		for (int q = 0; q < 9; q++) {
@@ -1660,7 +1666,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		la.rung = b->rung;
 		la.pot = b->pot;
 		la.kp = *kp;
-		la.compensated = 1;
+		la.compensated = c->compensated;
 		la.sums = counters + 4;
 		la.max_rung = c->d_flags + 48;
 		const bool fused = getenv("CT_LEAF_FUSED") != nullptr && b->nsub == 1 && !b->d_sub_h;
@@ -1708,7 +1714,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			}
 			pa.F = F;
 			pa.h = kp->h;
-			pa.compensated = 1;
+			pa.compensated = c->compensated;
 			pa.pairs = counters + 4 + 7;
 			pa.near_pairs = counters + 13;
 			// full tiles and tiles of at most 16 sinks go to separate launches

@@ -31,6 +31,25 @@ CT_HD_FN double ct_fma(double a, double b, double c) {
 	return std::fma(a, b, c);
 #endif
 }
+// Bit helpers for the Ewald image sets: population count, 1-based index of the lowest set
+// bit, and a word of a six-word register array chosen without dynamic indexing.
+CT_HD_FN int ct_popc(unsigned int m) {
+#ifdef __CUDA_ARCH__
+	return __popc(m);
+#else
+	return __builtin_popcount(m);
+#endif
+}
+CT_HD_FN int ct_ffs(unsigned int m) {
+#ifdef __CUDA_ARCH__
+	return __ffs((int) m);
+#else
+	return __builtin_ffs((int) m);
+#endif
+}
+CT_HD_FN unsigned int ct_word6(const unsigned int* a, int w) {
+	return w == 0 ? a[0] : w == 1 ? a[1] : w == 2 ? a[2] : w == 3 ? a[3] : w == 4 ? a[4] : a[5];
+}
 CT_HD_FN float ct_sqrt(float a) {
 #ifdef __CUDA_ARCH__
 	return __fsqrt_rn(a);

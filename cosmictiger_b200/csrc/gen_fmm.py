@@ -192,6 +192,13 @@ def emit_sum(em, target, terms, init, op="="):
             continue
         groups.setdefault(c, []).append(e)
     parts = []
+    lead = None
+    if init and 1 in groups:
+        # products with coefficient 1 go straight onto the initial value as fused multiply-adds
+        lead = init
+        for e in groups.pop(1):
+            lead = "ct_fma(%s, %s, %s)" % (e[0], e[1], lead) if isinstance(e, tuple) else "(%s + %s)" % (lead, e)
+        init = lead
     for c in sorted(groups, key=lambda c: (abs(c), c)):
         exprs = groups[c]
         # products are chained through explicit fused multiply-adds, so that host and device
@@ -580,7 +587,10 @@ def gen_header(P):
     h.append("#ifdef __CUDACC__")
     h.append("static __constant__ double ERF_SERIES_D[ORDER][ERF_SERIES_N] = {%s};" % body)
     h.append("#endif")
-    h.append(EWALD_TEMPLATE)
+    # Fourier accumulation unrolled: odd-order entries take the sine, even ones the cosine
+    acc = "\n".join("\t\tDf[%d] = ct_fma(%s, T(tab.four_exp[i][%d]), Df[%d]);" % (kk, "sn" if sum(n) & 1 else "cn", kk, kk)
+                    for kk, n in enumerate(tl_stored(P)))
+    h.append(EWALD_TEMPLATE.replace("@FOURIER_ACC@", acc))
     h.append("}  // namespace %s" % ns)
     return "\n".join(h) + "\n"
 
@@ -630,12 +640,40 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 			}
 		}
 	}
-	for (int i = 0; i < CT_EWALD_NREAL; i++) {
-		const T dx = x - T(1000) * T(tab.real[i][0]);
-		const T dy = y - T(1000) * T(tab.real[i][1]);
-		const T dz = z - T(1000) * T(tab.real[i][2]);
-		const T r2 = ct_fma(dx, dx, ct_fma(dy, dy, dz * dz));
-		if (r2 < T(1000 * 1000 * 2.6 * 2.6)) {
+	// Real images inside the cutoff: a first pass marks them in a bit set, the second evaluates
+	// them in increasing order.  Each thread then loops over its own images only, so the
+	// threads of a warp (each with its own separation) no longer step through the union of
+	// their image sets; the accumulation order is unchanged.
+	static_assert((CT_EWALD_NREAL + 31) / 32 == 6, "six words of image bits");
+	unsigned int inside[6];
+	int nin = 0;
+	for (int wd = 0; wd < 6; wd++) {
+		unsigned int m = 0u;
+		for (int b = 0; b < 32 && 32 * wd + b < CT_EWALD_NREAL; b++) {
+			const int i = 32 * wd + b;
+			const T dx = x - T(1000) * T(tab.real[i][0]);
+			const T dy = y - T(1000) * T(tab.real[i][1]);
+			const T dz = z - T(1000) * T(tab.real[i][2]);
+			const T r2 = ct_fma(dx, dx, ct_fma(dy, dy, dz * dz));
+			m |= (unsigned int) (r2 < T(1000 * 1000 * 2.6 * 2.6)) << b;
+		}
+		inside[wd] = m;
+		nin += ct_popc(m);
+	}
+	int wd = 0;
+	unsigned int bits = inside[0];
+	for (int q = 0; q < nin; q++) {
+		while (bits == 0u) {
+			wd++;
+			bits = ct_word6(inside, wd);
+		}
+		const int i = 32 * wd + ct_ffs(bits) - 1;
+		bits &= bits - 1u;
+		{
+			const T dx = x - T(1000) * T(tab.real[i][0]);
+			const T dy = y - T(1000) * T(tab.real[i][1]);
+			const T dz = z - T(1000) * T(tab.real[i][2]);
+			const T r2 = ct_fma(dx, dx, ct_fma(dy, dy, dz * dz));
 			icnt++;
 			const T r = ct_sqrt(r2);
 			const T rinv = T(1) / r;
@@ -660,10 +698,7 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 		const T hdotx = ct_fma(T(tab.four[i][0]), x, ct_fma(T(tab.four[i][1]), y, T(tab.four[i][2]) * z));
 		T sn, cn;
 		ct_sincos_poly(T(6.2831853071795865e-3) * hdotx, &sn, &cn);
-		for (int k = 0; k < NEXP; k++) {
-			const int order = CT_TAB(EXP_IDX)[k][0] + CT_TAB(EXP_IDX)[k][1] + CT_TAB(EXP_IDX)[k][2];
-			Df[k] = ct_fma((order & 1) ? sn : cn, T(tab.four_exp[i][k]), Df[k]);
-		}
+@FOURIER_ACC@
 	}
 	for (int i = 0; i < NEXP; i++) {
 		D[i] += Df[i];

@@ -220,6 +220,11 @@ ct_status ct_fp32_peak(ct_ctx* ctx, double* tflops);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own work with it. */
 void* ct_stream(ct_ctx* ctx);
 
+/* Summation of the per-sink particle-particle sums: 1 (default) adds the partial sums of the
+ * staged source batches with Neumaier compensation, 0 adds them plainly in FP32 (for precision
+ * studies; the reference adds plainly, gravity.cu:331-343). */
+ct_status ct_ctx_set_compensated(ct_ctx* ctx, int compensated);
+
 /* ---- allocation-free variant (no counterpart in the reference)
  *
  * For callers that cannot allocate device memory when they partition rungs: a host driver

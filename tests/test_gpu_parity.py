@@ -244,6 +244,18 @@ def test_ensemble_matches_separate_boxes(ctx):
         assert abs(krs[s].kin - kr.kin) <= 1e-9 * abs(kr.kin)
         b.close()
     ens.close()
+    # the context-wide return of an ensemble kick is the sum over its boxes
+    ens2 = ctx.ensemble(counts)
+    ens2.upload(*cat)
+    ens2.set_box_params(h, gms)
+    ens2.tree_create(theta, hh, 128)
+    kr_all = ens2.kick(kick_params(theta, hh, 1000))
+    nmom = sum(q.nmom for q in krs)
+    for f, scale in (("kin", None), ("pot", None), ("xmom", nmom), ("nmom", None)):
+        tot = sum(getattr(q, f) for q in krs)
+        assert abs(getattr(kr_all, f) - tot) <= 1e-9 * (scale if scale else abs(tot)), (f, getattr(kr_all, f), tot)
+    assert kr_all.max_rung == max(q.max_rung for q in krs)
+    ens2.close()
 
 
 def test_hierarchical_steps_match_oracle(ctx, oracle):
