@@ -38,6 +38,18 @@ template<> __device__ __forceinline__ const ct_p5::EwaldTab& ewald_tab<Ops5>() {
 	return c_tab5;
 }
 
+// The Ewald tables as the generated operator reads them, for kernels whose threads walk the
+// real images in different orders: the real-image vectors (indexed differently by every
+// thread) from a shared-memory copy, the Fourier terms and the r -> 0 limit (indexed alike by
+// all threads of a warp) from the __constant__ tables.
+template<class Tab>
+struct EwaldView {
+	const float (*real)[3];
+	const decltype(Tab::four)& four;
+	const decltype(Tab::four_exp)& four_exp;
+	const decltype(Tab::D0)& D0;
+};
+
 namespace {
 
 // ---------------------------------------------------------------- Ewald tables (FP64 on the device)
@@ -409,6 +421,13 @@ template<class Ops>
 __global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi, const int2* __restrict__ ecc,
 		const int* __restrict__ ecc_list, float* __restrict__ dL, int do_phi, double* counters) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
+	__shared__ float s_real[CT_EWALD_NREAL][3];
+	const auto& ct = ewald_tab<Ops>();
+	for (int i = threadIdx.x; i < CT_EWALD_NREAL * 3; i += blockDim.x) {
+		s_real[i / 3][i % 3] = ct.real[i / 3][i % 3];
+	}
+	__syncthreads();
+	const EwaldView<typename Ops::Tab> view { s_real, ct.four, ct.four_exp, ct.D0 };
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -441,7 +460,7 @@ __global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __re
 				if (4 * k + 2 < NM) M[4 * k + 2] = v.z;
 				if (4 * k + 3 < NM) M[4 * k + 3] = v.w;
 			}
-			const int ic = Ops::ewald(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z), ewald_tab<Ops>());
+			const int ic = Ops::ewald(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z), view);
 			icnt_tot += ic;
 			Ops::m2l(L, M, D, do_phi != 0);
 		}

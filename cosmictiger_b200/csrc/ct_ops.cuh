@@ -18,7 +18,7 @@ namespace ct {
 		template<class T> __host__ __device__ __forceinline__ static void greens_add(T* L, T x, T y, T z) { \
 			NS::greens_add(L, x, y, z);                                                                  \
 		}                                                                                                \
-		template<class T> __host__ __device__ __forceinline__ static int ewald(T* D, T x, T y, T z, const Tab& t) { \
+		template<class T, class TabT> __host__ __device__ __forceinline__ static int ewald(T* D, T x, T y, T z, const TabT& t) { \
 			return NS::ewald_greens(D, x, y, z, t);                                                      \
 		}                                                                                                \
 		template<class T> __host__ __device__ __forceinline__ static void m2l(T* L, const T* M, const T* D, bool p) { \
