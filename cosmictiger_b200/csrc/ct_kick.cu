@@ -418,10 +418,11 @@ __device__ __forceinline__ void warp_reduce_arr(float* L) {
 
 // Ewald M2L for every node: dL = sum over the Ewald CC list.
 template<class Ops>
-__global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi, const int2* __restrict__ ecc,
+__global__ void __launch_bounds__(128, 3) k_m2l_ewald(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi, const int2* __restrict__ ecc,
 		const int* __restrict__ ecc_list, float* __restrict__ dL, int do_phi, double* counters) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
 	__shared__ float s_real[CT_EWALD_NREAL][3];
+	__shared__ float s_L[4][32][51];
 	const auto& ct = ewald_tab<Ops>();
 	for (int i = threadIdx.x; i < CT_EWALD_NREAL * 3; i += blockDim.x) {
 		s_real[i / 3][i % 3] = ct.real[i / 3][i % 3];
@@ -443,7 +444,9 @@ __global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __re
 			continue;
 		}
 		const NodeW self = nodes[si];
-		float L[NE];
+		// this lane's expansion sum in shared memory (rows of 51 floats: lanes on distinct banks),
+		// which leaves the registers to the Green's function
+		float* L = &s_L[threadIdx.x >> 5][lane][0];
 		for (int i = 0; i < NE; i++) {
 			L[i] = 0.f;
 		}
@@ -451,6 +454,8 @@ __global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __re
 			const int c = ecc_list[lst.x + j];
 			const NodeW ot = nodes[c];
 			float M[NM], D[NE];
+			const int ic = Ops::ewald(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z), view);
+			icnt_tot += ic;
 			const float4* mp = (const float4*) (multi + (size_t) NMULT_STRIDE * c);
 #pragma unroll
 			for (int k = 0; k < (NM + 3) / 4; k++) {
@@ -460,16 +465,18 @@ __global__ void __launch_bounds__(128) k_m2l_ewald(int64_t nn, const NodeW* __re
 				if (4 * k + 2 < NM) M[4 * k + 2] = v.z;
 				if (4 * k + 3 < NM) M[4 * k + 3] = v.w;
 			}
-			const int ic = Ops::ewald(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z), view);
-			icnt_tot += ic;
 			Ops::m2l(L, M, D, do_phi != 0);
 		}
-		warp_reduce_arr<NE>(L);
-		if (lane == 0) {
-			for (int i = 0; i < NE; i++) {
-				dL[NEXP_STRIDE * si + i] = L[i];
+		__syncwarp();
+		// entry n summed over the 32 lanes' rows by lane n % 32
+		for (int n = lane; n < NE; n += 32) {
+			float t = 0.f;
+			for (int q = 0; q < 32; q++) {
+				t += s_L[threadIdx.x >> 5][q][n];
 			}
+			dL[NEXP_STRIDE * si + n] = t;
 		}
+		__syncwarp();
 	}
 	icnt_tot += __shfl_xor_sync(0xffffffffu, icnt_tot, 16);
 	icnt_tot += __shfl_xor_sync(0xffffffffu, icnt_tot, 8);

@@ -588,7 +588,7 @@ def gen_header(P):
     h.append("static __constant__ double ERF_SERIES_D[ORDER][ERF_SERIES_N] = {%s};" % body)
     h.append("#endif")
     # Fourier accumulation unrolled: odd-order entries take the sine, even ones the cosine
-    acc = "\n".join("\t\tDf[%d] = ct_fma(%s, T(tab.four_exp[i][%d]), Df[%d]);" % (kk, "sn" if sum(n) & 1 else "cn", kk, kk)
+    acc = "\n".join("\t\tD[%d] = ct_fma(%s, T(tab.four_exp[i][%d]), D[%d]);" % (kk, "sn" if sum(n) & 1 else "cn", kk, kk)
                     for kk, n in enumerate(tl_stored(P)))
     h.append(EWALD_TEMPLATE.replace("@FOURIER_ACC@", acc))
     h.append("}  // namespace %s" % ns)
@@ -690,18 +690,12 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 		}
 	}
 	detrace_full(D, Dr);
-	T Df[NEXP];
-	for (int i = 0; i < NEXP; i++) {
-		Df[i] = T(0);
-	}
+	// Fourier terms accumulate straight into the detraced real-space sum
 	for (int i = 0; i < CT_EWALD_NFOUR; i++) {
 		const T hdotx = ct_fma(T(tab.four[i][0]), x, ct_fma(T(tab.four[i][1]), y, T(tab.four[i][2]) * z));
 		T sn, cn;
 		ct_sincos_poly(T(6.2831853071795865e-3) * hdotx, &sn, &cn);
 @FOURIER_ACC@
-	}
-	for (int i = 0; i < NEXP; i++) {
-		D[i] += Df[i];
 	}
 	D[0] += T(7.8539816339744831e-4);
 	return icnt;
