@@ -144,6 +144,7 @@ def library():
     L.ct_box_download_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ct_sort_by_rung.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
     L.ct_ctx_set_compensated.argtypes = [vp, i32]
+    L.ct_ensemble_reshape.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
     L.ct_tree_create.argtypes = [vp, i32, ctypes.POINTER(TreeParams), ctypes.POINTER(i64)]
     L.ct_kick.argtypes = [vp, i32, ctypes.POINTER(KickParams), ctypes.POINTER(KickReturn)]
     L.ct_drift.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_double]
@@ -247,6 +248,16 @@ class Box:
         h = np.ascontiguousarray(h, np.float32)
         GM = np.ascontiguousarray(GM, np.float32)
         self.ctx.check(self.ctx.lib.ct_ensemble_set_params(self.ctx.h, self.id, _p(h), _p(GM)), "ct_ensemble_set_params")
+
+    def reshape(self, counts):
+        """Re-batch an ensemble in place for boxes of `counts` particles (ct_ensemble_reshape);
+        device arrays are reused while they are large enough."""
+        c = np.ascontiguousarray(counts, np.int64)
+        self.ctx.check(self.ctx.lib.ct_ensemble_reshape(self.ctx.h, self.id, len(c), c.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))),
+                       "ct_ensemble_reshape")
+        self.counts = c
+        self.n = int(np.sum(c))
+        self.tree_params = None
 
     def set_first_call(self, flags):
         f = np.ascontiguousarray(flags, np.int32)

@@ -618,6 +618,8 @@ static ct_status box_create_impl(Ctx* c, int nsub, const int64_t* counts, int* b
 		delete b;
 		return s;
 	}
+	b->cap = n;
+	b->sub_cap = nsub;
 	int id = -1;
 	for (size_t i = 0; i < c->boxes.size(); i++) {
 		if (!c->boxes[i]) {
@@ -663,8 +665,8 @@ ct_status ct_ensemble_set_params(ct_ctx* ctx, int box_id, const float* h, const 
 	}
 	cudaSetDevice(c->device);
 	if (!b->d_sub_h) {
-		CT_TRY(dalloc(c, (void**) &b->d_sub_h, sizeof(float) * b->nsub, "box softening"));
-		CT_TRY(dalloc(c, (void**) &b->d_sub_GM, sizeof(float) * b->nsub, "box GM"));
+		CT_TRY(dalloc(c, (void**) &b->d_sub_h, sizeof(float) * b->sub_cap, "box softening"));
+		CT_TRY(dalloc(c, (void**) &b->d_sub_GM, sizeof(float) * b->sub_cap, "box GM"));
 	}
 	b->sub_h_host.assign(h, h + b->nsub);
 	CT_CUDA(c, cudaMemcpy(b->d_sub_h, h, sizeof(float) * b->nsub, cudaMemcpyHostToDevice));
@@ -710,6 +712,92 @@ static ct_status ensemble_move(Ctx* c, int ens_id, const int* boxes, int count, 
 	return CT_OK;
 }
 
+ct_status ct_ensemble_reshape(ct_ctx* ctx, int box_id, int nbox, const int64_t* counts) {
+	Ctx* c = (Ctx*) ctx;
+	Box* b = get_box(c, box_id);
+	if (!b || nbox < 1 || !counts) {
+		return fail(c, CT_ERR_ARG, "ct_ensemble_reshape: bad arguments");
+	}
+	int64_t n = 0;
+	for (int s = 0; s < nbox; s++) {
+		if (counts[s] < 0) {
+			return fail(c, CT_ERR_ARG, "ct_ensemble_reshape: negative particle count");
+		}
+		n += counts[s];
+	}
+	if (n > (int64_t) INT32_MAX / 2) {
+		return fail(c, CT_ERR_ARG, "ct_ensemble_reshape: too many particles for 32-bit indices");
+	}
+	cudaSetDevice(c->device);
+	CT_CUDA(c, cudaStreamSynchronize(c->stream));
+	if (n > b->cap) {
+		// particle arrays grow with headroom; their contents are replaced by the caller
+		const int64_t cap = std::max<int64_t>(n, b->cap + b->cap / 2);
+		for (int d = 0; d < 3; d++) {
+			dfree(c, b->x[d], sizeof(uint32_t) * b->cap);
+			dfree(c, b->v[d], sizeof(float) * b->cap);
+			dfree(c, b->g[d], sizeof(float) * b->g_cap);
+			b->x[d] = nullptr;
+			b->g[d] = nullptr;
+			b->v[d] = nullptr;
+		}
+		dfree(c, b->pot, sizeof(float) * b->g_cap);
+		dfree(c, b->rung, b->cap + 16);
+		b->pot = nullptr;
+		b->rung = nullptr;
+		b->g_cap = 0;
+		b->cap = 0;
+		for (int d = 0; d < 3; d++) {
+			CT_TRY(dalloc(c, (void**) &b->x[d], sizeof(uint32_t) * cap, "positions"));
+			CT_TRY(dalloc(c, (void**) &b->v[d], sizeof(float) * cap, "velocities"));
+		}
+		CT_TRY(dalloc(c, (void**) &b->rung, cap + 16, "rungs"));
+		b->cap = cap;
+	}
+	if (nbox > b->sub_cap) {
+		const int sc = std::max(nbox, b->sub_cap + b->sub_cap / 2);
+		dfree(c, b->d_sub_off, sizeof(int64_t) * (b->sub_cap + 1));
+		dfree(c, b->d_sub_sums, sizeof(double) * 9 * b->sub_cap);
+		dfree(c, b->d_sub_maxrung, sizeof(int) * b->sub_cap);
+		dfree(c, b->d_sub_h, sizeof(float) * b->sub_cap);
+		dfree(c, b->d_sub_GM, sizeof(float) * b->sub_cap);
+		dfree(c, b->d_sub_first, sizeof(int) * b->sub_cap);
+		b->d_sub_off = nullptr;
+		b->d_sub_sums = nullptr;
+		b->d_sub_maxrung = nullptr;
+		b->d_sub_h = b->d_sub_GM = nullptr;
+		b->d_sub_first = nullptr;
+		b->sub_cap = 0;
+		CT_TRY(dalloc(c, (void**) &b->d_sub_off, sizeof(int64_t) * (sc + 1), "box offsets"));
+		CT_TRY(dalloc(c, (void**) &b->d_sub_sums, sizeof(double) * 9 * sc, "box sums"));
+		CT_TRY(dalloc(c, (void**) &b->d_sub_maxrung, sizeof(int) * sc, "box max rungs"));
+		b->sub_cap = sc;
+	}
+	b->n = n;
+	b->nsub = nbox;
+	b->sub_off.assign(nbox + 1, 0);
+	for (int s = 0; s < nbox; s++) {
+		b->sub_off[s + 1] = b->sub_off[s] + counts[s];
+	}
+	CT_CUDA(c, cudaMemcpy(b->d_sub_off, b->sub_off.data(), sizeof(int64_t) * (nbox + 1), cudaMemcpyHostToDevice));
+	// the per-box softening, GM and first-call flags of the old layout no longer apply
+	if (b->d_sub_h) {
+		b->sub_h_host.clear();
+		dfree(c, b->d_sub_h, sizeof(float) * b->sub_cap);
+		dfree(c, b->d_sub_GM, sizeof(float) * b->sub_cap);
+		b->d_sub_h = b->d_sub_GM = nullptr;
+	}
+	if (b->d_sub_first) {
+		dfree(c, b->d_sub_first, sizeof(int) * b->sub_cap);
+		b->d_sub_first = nullptr;
+	}
+	b->rung_begin = 0;
+	b->rung_stack.clear();
+	b->tree_valid = false;
+	b->have_force = false;
+	return CT_OK;
+}
+
 ct_status ct_ensemble_set_first_call(ct_ctx* ctx, int box_id, const int* first_call) {
 	Ctx* c = (Ctx*) ctx;
 	Box* b = get_box(c, box_id);
@@ -718,7 +806,7 @@ ct_status ct_ensemble_set_first_call(ct_ctx* ctx, int box_id, const int* first_c
 	}
 	cudaSetDevice(c->device);
 	if (!b->d_sub_first) {
-		CT_TRY(dalloc(c, (void**) &b->d_sub_first, sizeof(int) * b->nsub, "box first-call flags"));
+		CT_TRY(dalloc(c, (void**) &b->d_sub_first, sizeof(int) * b->sub_cap, "box first-call flags"));
 	}
 	CT_CUDA(c, cudaMemcpy(b->d_sub_first, first_call, sizeof(int) * b->nsub, cudaMemcpyHostToDevice));
 	return CT_OK;
@@ -748,13 +836,13 @@ ct_status ct_box_destroy(ct_ctx* ctx, int box_id) {
 		return fail(c, CT_ERR_ARG, "ct_box_destroy: no such box");
 	}
 	cudaStreamSynchronize(c->stream);
-	const int64_t n = b->n;
+	const int64_t n = b->cap;
 	for (int d = 0; d < 3; d++) {
 		dfree(c, b->x[d], sizeof(uint32_t) * n);
 		dfree(c, b->v[d], sizeof(float) * n);
-		dfree(c, b->g[d], sizeof(float) * n);
+		dfree(c, b->g[d], sizeof(float) * b->g_cap);
 	}
-	dfree(c, b->pot, sizeof(float) * n);
+	dfree(c, b->pot, sizeof(float) * b->g_cap);
 	dfree(c, b->rung, n + 16);
 	const int64_t cap = b->node_cap;
 	dfree(c, b->nodes, sizeof(NodeW) * cap);
@@ -765,12 +853,12 @@ ct_status ct_box_destroy(ct_ctx* ctx, int box_id) {
 	dfree(c, b->parent, sizeof(int32_t) * cap);
 	dfree(c, b->gbox, sizeof(double) * 6 * cap);
 	dfree(c, b->tbox, sizeof(double) * 6 * cap);
-	dfree(c, b->d_sub_off, sizeof(int64_t) * (b->nsub + 1));
-	dfree(c, b->d_sub_sums, sizeof(double) * 9 * b->nsub);
-	dfree(c, b->d_sub_maxrung, sizeof(int) * b->nsub);
-	dfree(c, b->d_sub_h, sizeof(float) * b->nsub);
-	dfree(c, b->d_sub_GM, sizeof(float) * b->nsub);
-	dfree(c, b->d_sub_first, sizeof(int) * b->nsub);
+	dfree(c, b->d_sub_off, sizeof(int64_t) * (b->sub_cap + 1));
+	dfree(c, b->d_sub_sums, sizeof(double) * 9 * b->sub_cap);
+	dfree(c, b->d_sub_maxrung, sizeof(int) * b->sub_cap);
+	dfree(c, b->d_sub_h, sizeof(float) * b->sub_cap);
+	dfree(c, b->d_sub_GM, sizeof(float) * b->sub_cap);
+	dfree(c, b->d_sub_first, sizeof(int) * b->sub_cap);
 	delete b;
 	c->boxes[box_id] = nullptr;
 	return CT_OK;
@@ -936,11 +1024,19 @@ ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick
 		return fail(c, CT_ERR_ARG, "ct_kick: theta differs from the one the tree was built with");
 	}
 	cudaSetDevice(c->device);
-	if (params->save_force && !b->pot) {
+	if (params->save_force && (!b->pot || b->g_cap < b->n)) {
 		for (int d = 0; d < 3; d++) {
-			CT_TRY(dalloc(c, (void**) &b->g[d], sizeof(float) * b->n, "forces"));
+			dfree(c, b->g[d], sizeof(float) * b->g_cap);
+			b->g[d] = nullptr;
 		}
-		CT_TRY(dalloc(c, (void**) &b->pot, sizeof(float) * b->n, "potentials"));
+		dfree(c, b->pot, sizeof(float) * b->g_cap);
+		b->pot = nullptr;
+		b->g_cap = 0;
+		for (int d = 0; d < 3; d++) {
+			CT_TRY(dalloc(c, (void**) &b->g[d], sizeof(float) * b->cap, "forces"));
+		}
+		CT_TRY(dalloc(c, (void**) &b->pot, sizeof(float) * b->cap, "potentials"));
+		b->g_cap = b->cap;
 	}
 	return kick_run(c, b, params, result);
 }

@@ -75,6 +75,9 @@ struct Ctx;
 // Per-box device state.
 struct Box {
 	int64_t n = 0;
+	int64_t cap = 0;         // particles the x, v, rung arrays hold
+	int64_t g_cap = 0;       // particles the g, pot arrays hold
+	int sub_cap = 0;         // sub-boxes the per-box arrays hold
 	int64_t rung_begin = 0;  // tree covers [rung_begin, n)
 	// particles (SoA)
 	uint32_t* x[3] = { nullptr, nullptr, nullptr };

@@ -92,13 +92,15 @@ class Server:
     def _ensemble(self):
         members = [r.rid for r, _, _ in self.active]
         if members != self.ens_members:
-            if self.ens is not None:
-                if self.ens_dirty:
-                    # members still running keep their advanced state across the rebuild
-                    self.ens.scatter(self.ens_boxes)
-                self.ens.close()
             counts = [r.particles for r, _, _ in self.active]
-            self.ens = self.ctx.ensemble(counts)
+            if self.ens is None:
+                self.ens = self.ctx.ensemble(counts)
+            else:
+                if self.ens_dirty:
+                    # members still running keep their advanced state across the re-batch
+                    self.ens.scatter(self.ens_boxes)
+                # one ensemble for the whole run, re-batched in place (device arrays reused)
+                self.ens.reshape(counts)
             h = np.array([ics.softening(c, 0.02) for c in counts], np.float32)
             gm = np.array([1.0 / c for c in counts], np.float32)
             self.ens.set_box_params(h, gm)

@@ -130,6 +130,11 @@ ct_status ct_ensemble_create(ct_ctx* ctx, int nbox, const int64_t* counts, int* 
 /* Per-box softening h and GM of an ensemble (box s: h[s], GM[s]); without this call every box
  * uses the kick's h and GM.  The tree build's leaf criterion uses the tree parameters' hsoft. */
 ct_status ct_ensemble_set_params(ct_ctx* ctx, int box_id, const float* h, const float* GM);
+/* New membership for an existing ensemble: nbox boxes of counts[0..nbox) particles.  Device
+ * arrays are kept and grown only when the new totals exceed what they hold, so a serving loop
+ * can re-batch every step without reallocating; particle contents, per-box parameters and
+ * first-call flags are undefined afterwards (gather or upload, set_params, set_first_call). */
+ct_status ct_ensemble_reshape(ct_ctx* ctx, int box_id, int nbox, const int64_t* counts);
 /* Per-box first_call flags of an ensemble (boxes joining a batch start their own runs). */
 ct_status ct_ensemble_set_first_call(ct_ctx* ctx, int box_id, const int* first_call);
 /* Copy the particles of plain boxes boxes[0..count) into the ensemble's slots (gather) or

@@ -258,6 +258,37 @@ def test_ensemble_matches_separate_boxes(ctx):
     ens2.close()
 
 
+def test_ensemble_reshape_matches_fresh_ensemble(ctx):
+    """An ensemble re-batched in place (ct_ensemble_reshape: more boxes, more particles, then
+    fewer) gives bit-identical trees and forces to a freshly created ensemble."""
+    first = [lattice(10, seed=31), lattice(8, seed=32)]
+    second = [lattice(12, seed=33), ics.clustered_box(9, nspheres=4, seed=34), lattice(7, seed=35)]
+    third = [lattice(9, seed=36)]
+    theta = 0.55
+    ens = ctx.ensemble([len(s[0]) for s in first])
+    for sets in (first, second, third):
+        counts = [len(s[0]) for s in sets]
+        h = [ics.softening(n, 0.02) for n in counts]
+        cat = [np.concatenate([s[k] for s in sets]) for k in range(5)]
+        if sets is not first:
+            ens.reshape(counts)
+        ens.upload(*cat)
+        ens.set_box_params(h, [1.0 / n for n in counts])
+        ens.tree_create(theta, min(h), 128)
+        ens.kick(kick_params(theta, min(h), 1000))
+        got = ens.download(forces=True)
+        fresh = ctx.ensemble(counts)
+        fresh.upload(*cat)
+        fresh.set_box_params(h, [1.0 / n for n in counts])
+        fresh.tree_create(theta, min(h), 128)
+        fresh.kick(kick_params(theta, min(h), 1000))
+        want = fresh.download(forces=True)
+        fresh.close()
+        for f in ("x", "y", "z", "v", "rung", "gx", "gy", "gz", "pot"):
+            assert np.array_equal(got[f], want[f]), (len(sets), f)
+    ens.close()
+
+
 def test_hierarchical_steps_match_oracle(ctx, oracle):
     """Three multistep steps (the rung ladder of kick_step_hierarchical) on the device and in
     the oracle from the same clustered start: same ladder, rungs, positions and velocities."""

@@ -21,13 +21,18 @@ class FakeBox:
 
 
 class FakeEnsemble:
-    def __init__(self, counts, log):
+    def __init__(self, counts, log, peak):
         self.slots = [0] * len(counts)
         self.first = None
         self.log = log
+        self.ctx_peak = peak
 
     def set_box_params(self, h, gm):
         pass
+
+    def reshape(self, counts):
+        self.slots = [None] * len(counts)  # contents undefined until the next gather
+        self.ctx_peak(counts)
 
     def gather(self, boxes):
         assert not any(b.closed for b in boxes)
@@ -64,9 +69,12 @@ class FakeContext:
     def box(self, n):
         return FakeBox(n)
 
-    def ensemble(self, counts):
+    def note(self, counts):
         self.peak = max(self.peak, sum(counts))
-        return FakeEnsemble(counts, self.log)
+
+    def ensemble(self, counts):
+        self.note(counts)
+        return FakeEnsemble(counts, self.log, self.note)
 
     def synchronize(self):
         pass
