@@ -1068,57 +1068,63 @@ template<bool CHECK>
 __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int jb, int je, float kx, float ky, float kz, float h2, float hinv,
 		float h2inv, float h3inv, float& fx, float& fy, float& fz, float& pt) {
 	int j = jb;
-	if (!CHECK) {
-		const f2 KX = f2_pack(kx, kx), KY = f2_pack(ky, ky), KZ = f2_pack(kz, kz);
-		f2 ax = f2_pack(0.f, 0.f), ay = ax, az = ax, ap = ax;
-		// four sources (two f32x2 pairs) starting at q, a multiple of 4
-		auto quad = [&](int q) {
-			const float4 xy0 = st->xy[q >> 1];
-			const float4 xy1 = st->xy[(q >> 1) + 1];
-			const float4 zz = st->z[q >> 2];
-			const f2 dx0 = f2_sub(KX, f2_pack(xy0.x, xy0.y)), dy0 = f2_sub(KY, f2_pack(xy0.z, xy0.w)), dz0 = f2_sub(KZ, f2_pack(zz.x, zz.y));
-			const f2 dx1 = f2_sub(KX, f2_pack(xy1.x, xy1.y)), dy1 = f2_sub(KY, f2_pack(xy1.z, xy1.w)), dz1 = f2_sub(KZ, f2_pack(zz.z, zz.w));
-			const f2 q0 = f2_fma(dx0, dx0, f2_fma(dy0, dy0, f2_mul(dz0, dz0)));
-			const f2 q1 = f2_fma(dx1, dx1, f2_fma(dy1, dy1, f2_mul(dz1, dz1)));
-			float a0, b0, a1, b1;
-			f2_unpack(q0, a0, b0);
-			f2_unpack(q1, a1, b1);
-			const f2 r10 = f2_pack(rsqrt_ftz(a0), rsqrt_ftz(b0));
-			const f2 r11 = f2_pack(rsqrt_ftz(a1), rsqrt_ftz(b1));
-			const f2 r30 = f2_mul(f2_mul(r10, r10), r10);
-			const f2 r31 = f2_mul(f2_mul(r11, r11), r11);
-			ax = f2_fma(dx0, r30, ax);
-			ay = f2_fma(dy0, r30, ay);
-			az = f2_fma(dz0, r30, az);
-			ap = f2_sub(ap, r10);
-			ax = f2_fma(dx1, r31, ax);
-			ay = f2_fma(dy1, r31, ay);
-			az = f2_fma(dz1, r31, az);
-			ap = f2_sub(ap, r11);
-		};
-		if (jb == 0 && je == P2P_STAGE) {
-			// a full chunk: constant offsets, no loop arithmetic
-#pragma unroll
-			for (int q = 0; q < P2P_STAGE; q += 4) {
-				quad(q);
+	const f2 KX = f2_pack(kx, kx), KY = f2_pack(ky, ky), KZ = f2_pack(kz, kz);
+	f2 ax = f2_pack(0.f, 0.f), ay = ax, az = ax, ap = ax;
+	// four sources (two f32x2 pairs) starting at q, a multiple of 4.  With CHECK, a quad with
+	// a pair inside the softening length goes through the scalar per-pair test instead (rare:
+	// near source leaves mostly hold pairs farther apart than h).
+	auto quad = [&](int q) {
+		const float4 xy0 = st->xy[q >> 1];
+		const float4 xy1 = st->xy[(q >> 1) + 1];
+		const float4 zz = st->z[q >> 2];
+		const f2 dx0 = f2_sub(KX, f2_pack(xy0.x, xy0.y)), dy0 = f2_sub(KY, f2_pack(xy0.z, xy0.w)), dz0 = f2_sub(KZ, f2_pack(zz.x, zz.y));
+		const f2 dx1 = f2_sub(KX, f2_pack(xy1.x, xy1.y)), dy1 = f2_sub(KY, f2_pack(xy1.z, xy1.w)), dz1 = f2_sub(KZ, f2_pack(zz.z, zz.w));
+		const f2 q0 = f2_fma(dx0, dx0, f2_fma(dy0, dy0, f2_mul(dz0, dz0)));
+		const f2 q1 = f2_fma(dx1, dx1, f2_fma(dy1, dy1, f2_mul(dz1, dz1)));
+		float a0, b0, a1, b1;
+		f2_unpack(q0, a0, b0);
+		f2_unpack(q1, a1, b1);
+		if (CHECK && !(fminf(fminf(a0, b0), fminf(a1, b1)) > h2)) {
+			for (int t = 0; t < 4; t++) {
+				p2p_checked(st, q + t, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 			}
-			j = P2P_STAGE;
-		} else {
-#pragma unroll 2
-			for (; j + 3 < je; j += 4) {
-				quad(j);
-			}
+			return;
 		}
-		float lo, hi;
-		f2_unpack(ax, lo, hi);
-		fx += lo + hi;
-		f2_unpack(ay, lo, hi);
-		fy += lo + hi;
-		f2_unpack(az, lo, hi);
-		fz += lo + hi;
-		f2_unpack(ap, lo, hi);
-		pt += lo + hi;
+		const f2 r10 = f2_pack(rsqrt_ftz(a0), rsqrt_ftz(b0));
+		const f2 r11 = f2_pack(rsqrt_ftz(a1), rsqrt_ftz(b1));
+		const f2 r30 = f2_mul(f2_mul(r10, r10), r10);
+		const f2 r31 = f2_mul(f2_mul(r11, r11), r11);
+		ax = f2_fma(dx0, r30, ax);
+		ay = f2_fma(dy0, r30, ay);
+		az = f2_fma(dz0, r30, az);
+		ap = f2_sub(ap, r10);
+		ax = f2_fma(dx1, r31, ax);
+		ay = f2_fma(dy1, r31, ay);
+		az = f2_fma(dz1, r31, az);
+		ap = f2_sub(ap, r11);
+	};
+	if (!CHECK && jb == 0 && je == P2P_STAGE) {
+		// a full chunk: constant offsets, no loop arithmetic
+#pragma unroll
+		for (int q = 0; q < P2P_STAGE; q += 4) {
+			quad(q);
+		}
+		j = P2P_STAGE;
+	} else {
+#pragma unroll 2
+		for (; j + 3 < je; j += 4) {
+			quad(j);
+		}
 	}
+	float lo, hi;
+	f2_unpack(ax, lo, hi);
+	fx += lo + hi;
+	f2_unpack(ay, lo, hi);
+	fy += lo + hi;
+	f2_unpack(az, lo, hi);
+	fz += lo + hi;
+	f2_unpack(ap, lo, hi);
+	pt += lo + hi;
 	for (; j < je; j++) {
 		p2p_checked(st, j, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 	}
