@@ -659,13 +659,16 @@ def study_precision(args, torch):
 
 def study_ensemble(args, torch):
     """512 independent boxes, n_i log-uniform in [16, 128], own Zel'dovich fields, theta 0.55,
-    20 steps: one batched ensemble vs the plain single-box path launched box by box."""
+    20 steps (or the --ensemble-* sizes when given): one batched ensemble vs the plain
+    single-box path launched box by box."""
     import cosmictiger_b200 as ct
 
     ctx = ct.Context(order=7)
     lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
     a = argparse.Namespace(**vars(args))
-    a.ensemble_boxes, a.ensemble_nmin, a.ensemble_nmax, a.ensemble_steps = 512, 16, 128, 20
+    if (args.ensemble_boxes, args.ensemble_nmin, args.ensemble_nmax, args.ensemble_steps) == (64, 16, 64, 3):
+        # sizes left at the benchmark line's defaults: the study's own configuration
+        a.ensemble_boxes, a.ensemble_nmin, a.ensemble_nmax, a.ensemble_steps = 512, 16, 128, 20
     res = ensemble_compare(ct, torch, ctx, a, args.theta, lib_stream)
     ctx.close()
     return {"study": "ensemble", **res}
