@@ -646,33 +646,8 @@ __global__ void k_l2l(int64_t lb, int64_t le, const NodeW* __restrict__ nodes, c
 	}
 }
 
-// ---------------------------------------------------------------- leaf kernel
-constexpr int LEAF_TPB = 128;
-constexpr int PP_BATCH = 1024;
-
-struct LeafArgs {
-	const NodeW* nodes;
-	const float* multi;
-	const float* Lx;
-	const int64_t* leaves;
-	int64_t nleaves;
-	const int2* pc;
-	const int* pc_list;
-	const int2* pp;
-	const int* pp_list;
-	const uint32_t* x[3];
-	float* v[3];
-	int8_t* rung;
-	float* g[3];
-	float* pot;
-	ct_kick_params kp;
-	int compensated;
-	double* sums;  // [0] pot [1] kin [2] dkin [3] xmom [4] ymom [5] zmom [6] nmom [7] pp pairs [8] pc pairs
-	int* max_rung;
-};
-
+// Neumaier-compensated running sum of per-batch partial forces.
 __device__ __forceinline__ void ksum(float& s, float& comp, float v) {
-	// Neumaier-compensated running sum of per-batch partial forces
 	const float t = s + v;
 	if (fabsf(s) >= fabsf(v)) {
 		comp += (s - t) + v;
@@ -682,244 +657,9 @@ __device__ __forceinline__ void ksum(float& s, float& comp, float v) {
 	s = t;
 }
 
-template<class Ops>
-__global__ void __launch_bounds__(LEAF_TPB) k_leaf(LeafArgs a) {
-	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
-	__shared__ float4 src[PP_BATCH];
-	__shared__ float s_mp[NM];
-	__shared__ uint32_t s_mpos[3];
-	__shared__ double s_red[LEAF_TPB / 32][9];
-	const int tid = threadIdx.x;
-	const auto& kp = a.kp;
-	const float h = kp.h;
-	const float h2 = h * h;
-	const float hinv = 1.f / h;
-	const float h2inv = hinv * hinv;
-	const float h3inv = h2inv * hinv;
-	const float self_phi = 693.f / 256.f;
-	double acc[9];
-	for (int k = 0; k < 9; k++) {
-		acc[k] = 0.0;
-	}
-	int maxr = 0;
-	for (int64_t li = blockIdx.x; li < a.nleaves; li += gridDim.x) {
-		const int64_t si = a.leaves[li];
-		const NodeW self = a.nodes[si];
-		const int nsink = self.pend - self.pbeg;
-		const int2 ppl = a.pp[si];
-		const int2 pcl = a.pc[si];
-		for (int s0 = 0; s0 < nsink; s0 += LEAF_TPB) {
-			const int k = s0 + tid;
-			const bool active = k < nsink;
-			const int snk = self.pbeg + k;
-			uint32_t X[3] = { self.x, self.y, self.z };
-			if (active) {
-				X[0] = a.x[0][snk];
-				X[1] = a.x[1][snk];
-				X[2] = a.x[2][snk];
-			}
-			// sink relative to the leaf centre
-			const float kx = fixed_dist(X[0], self.x), ky = fixed_dist(X[1], self.y), kz = fixed_dist(X[2], self.z);
-			float Fx = 0.f, Fy = 0.f, Fz = 0.f, Fp = self_phi * hinv;
-			// ---- M2P (gravity.cu:157-211): source multipoles at this sink
-			for (int q = 0; q < pcl.y; q++) {
-				const int c = a.pc_list[pcl.x + q];
-				__syncthreads();
-				if (tid < NM) {
-					s_mp[tid] = a.multi[(size_t) NMULT_STRIDE * c + tid];
-				}
-				if (tid == 0) {
-					const NodeW ot = a.nodes[c];
-					s_mpos[0] = ot.x;
-					s_mpos[1] = ot.y;
-					s_mpos[2] = ot.z;
-				}
-				__syncthreads();
-				if (active) {
-					float D[NE], M[NM], L2[5] = { 0.f, 0.f, 0.f, 0.f, 0.f };
-					for (int i = 0; i < NM; i++) {
-						M[i] = s_mp[i];
-					}
-					Ops::greens(D, fixed_dist(X[0], s_mpos[0]), fixed_dist(X[1], s_mpos[1]), fixed_dist(X[2], s_mpos[2]));
-					Ops::m2l2(L2, M, D, kp.do_phi != 0);
-					Fx -= 1e6f * L2[1];
-					Fy -= 1e6f * L2[2];
-					Fz -= 1e6f * L2[3];
-					Fp += 1e3f * L2[0];
-				}
-			}
-			if (active) {
-				acc[8] += pcl.y;
-			}
-			// ---- P2P (gravity.cu:246-404)
-			float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-			float cx = 0.f, cy = 0.f, cz = 0.f, cpot = 0.f;
-			int q = 0;          // index in the P2P list
-			int qoff = 0;       // particles of list entry q already staged
-			int64_t npairs = 0;
-			while (q < ppl.y) {
-				__syncthreads();
-				// stage up to PP_BATCH sources (relative to the leaf centre)
-				int nb = 0;
-				while (nb < PP_BATCH && q < ppl.y) {
-					const NodeW ot = a.nodes[a.pp_list[ppl.x + q]];
-					const int avail = (ot.pend - ot.pbeg) - qoff;
-					const int take = min(avail, PP_BATCH - nb);
-					for (int j = tid; j < take; j += LEAF_TPB) {
-						const int pi = ot.pbeg + qoff + j;
-						src[nb + j] = make_float4(fixed_dist(a.x[0][pi], self.x), fixed_dist(a.x[1][pi], self.y), fixed_dist(a.x[2][pi], self.z), 0.f);
-					}
-					nb += take;
-					qoff += take;
-					if (qoff == ot.pend - ot.pbeg) {
-						q++;
-						qoff = 0;
-					}
-				}
-				__syncthreads();
-				if (active) {
-					float fx = 0.f, fy = 0.f, fz = 0.f, pt = 0.f;
-					for (int j = 0; j < nb; j++) {
-						const float4 s = src[j];
-						const float dx = kx - s.x, dy = ky - s.y, dz = kz - s.z;
-						const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-						float r1inv, r3inv;
-						if (r2 > h2) {
-							r1inv = rsqrtf(r2);
-							r3inv = r1inv * r1inv * r1inv;
-						} else {
-							// Ferrer softening kernel (gravity.hpp:73-96)
-							const float q2 = r2 * h2inv;
-							float f = 315.f / 128.f;
-							f = fmaf(f, q2, -385.f / 32.f);
-							f = fmaf(f, q2, 1485.f / 64.f);
-							f = fmaf(f, q2, -693.f / 32.f);
-							f = fmaf(f, q2, 1155.f / 128.f);
-							r3inv = f * h3inv;
-							float ph = -63.f / 256.f;
-							ph = fmaf(ph, q2, 385.f / 256.f);
-							ph = fmaf(ph, q2, -495.f / 128.f);
-							ph = fmaf(ph, q2, 693.f / 128.f);
-							ph = fmaf(ph, q2, -1155.f / 256.f);
-							ph = fmaf(ph, q2, 693.f / 256.f);
-							r1inv = ph * hinv;
-						}
-						fx = fmaf(dx, r3inv, fx);
-						fy = fmaf(dy, r3inv, fy);
-						fz = fmaf(dz, r3inv, fz);
-						pt -= r1inv;
-					}
-					if (a.compensated) {
-						ksum(sx, cx, fx);
-						ksum(sy, cy, fy);
-						ksum(sz, cz, fz);
-						ksum(sp, cpot, pt);
-					} else {
-						sx += fx;
-						sy += fy;
-						sz += fz;
-						sp += pt;
-					}
-					npairs += nb;
-				}
-			}
-			if (active) {
-				Fx -= sx + cx;
-				Fy -= sy + cy;
-				Fz -= sz + cz;
-				Fp += sp + cpot;
-				acc[7] += (double) npairs;
-				// ---- L2P and the kick (kick.cu:53-177)
-				float La[NE], L2[5];
-				const float* Lsrc = a.Lx + (size_t) NEXP_STRIDE * si;
-				for (int i = 0; i < NE; i++) {
-					La[i] = Lsrc[i];
-				}
-				Ops::l2p(L2, La, kx, ky, kz, kp.do_phi != 0);
-				Fp += 1e3f * L2[0];
-				Fx -= 1e6f * L2[1];
-				Fy -= 1e6f * L2[2];
-				Fz -= 1e6f * L2[3];
-				Fz *= kp.GM;
-				Fy *= kp.GM;
-				Fx *= kp.GM;
-				Fp *= kp.GM;
-				float vx = a.v[0][snk], vy = a.v[1][snk], vz = a.v[2][snk];
-				const float kin0 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
-				const float sgn = kp.sign * (kp.top ? 1.f : -1.f);
-				const float rdt = 1.0f / (float) (1 << kp.min_rung);
-				if (kp.ascending) {
-					const float dt = 0.5f * rdt * kp.t0;
-					if (!kp.first_call) {
-						vx = fmaf(sgn * Fx, dt, vx);
-						vy = fmaf(sgn * Fy, dt, vy);
-						vz = fmaf(sgn * Fz, dt, vz);
-					}
-				}
-				acc[1] += 0.5f * (vx * vx + vy * vy + vz * vz);
-				acc[3] += vx;
-				acc[4] += vy;
-				acc[5] += vz;
-				acc[6] += sqrtf(vx * vx + vy * vy + vz * vz);
-				if (kp.save_force) {
-					a.g[0][snk] = Fx;
-					a.g[1][snk] = Fy;
-					a.g[2][snk] = Fz;
-					a.pot[snk] = Fp;
-				}
-				if (kp.descending) {
-					const float g2 = Fx * Fx + Fy * Fy + Fz * Fz;
-					float dt = fminf(kp.eta * sqrtf(kp.a * h * rsqrtf(g2)), kp.t0);
-					dt = fminf(kp.max_dt, dt);
-					int r = a.rung[snk];
-					r = max(kp.min_rung + int((int) ceilf(log2f(kp.t0 / dt)) > kp.min_rung), r - 1);
-					r = max(0, min(r, 15));
-					a.rung[snk] = (int8_t) r;
-					maxr = max(maxr, r);
-					dt = 0.5f * rdt * kp.t0;
-					vx = fmaf(sgn * Fx, dt, vx);
-					vy = fmaf(sgn * Fy, dt, vy);
-					vz = fmaf(sgn * Fz, dt, vz);
-				}
-				const float kin1 = (float) (0.5 * (double) (vx * vx + vy * vy + vz * vz));
-				a.v[0][snk] = vx;
-				a.v[1][snk] = vy;
-				a.v[2][snk] = vz;
-				acc[0] += 0.5f * Fp;
-				acc[2] += kin1 - kin0;
-			}
-		}
-	}
-	// block reduction of the sums
-	const int lane = tid & 31, w = tid >> 5;
-	for (int k = 0; k < 9; k++) {
-		double v = acc[k];
-		for (int o = 16; o; o >>= 1) {
-			v += __shfl_xor_sync(0xffffffffu, v, o);
-		}
-		if (lane == 0) {
-			s_red[w][k] = v;
-		}
-	}
-	for (int o = 16; o; o >>= 1) {
-		maxr = max(maxr, __shfl_xor_sync(0xffffffffu, maxr, o));
-	}
-	__syncthreads();
-	if (tid < 9) {
-		double v = 0;
-		for (int q = 0; q < LEAF_TPB / 32; q++) {
-			v += s_red[q][tid];
-		}
-		atomicAdd(a.sums + tid, v);
-	}
-	if (lane == 0 && maxr > 0) {
-		atomicMax(a.max_rung, maxr);
-	}
-}
-
-// ---------------------------------------------------------------- split leaf path
-// P2P alone (warp per 32-sink tile of a leaf, sources staged per warp in shared memory as
-// float4 positions relative to the leaf centre), then M2P + L2P + kick per tile.
+// ---------------------------------------------------------------- leaf path
+// P2P (a warp per 32-sink tile of a leaf; the particles of its P2P source leaves staged per
+// warp in shared memory as offsets from the leaf centre), then M2P + L2P + kick per tile.
 constexpr int P2P_TPB = 256;
 constexpr int P2P_STAGE = 128;
 
@@ -1680,36 +1420,10 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		CT_CUDA(c, cudaMemcpyAsync(hf, lcount, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
 		CT_CUDA(c, cudaStreamSynchronize(st));
 		const int64_t nleaves = (int64_t) * (unsigned long long*) hf;
-		LeafArgs la;
-		la.nodes = b->nodes;
-		la.multi = b->multi;
-		la.Lx = K.Lx;
-		la.leaves = K.leaves;
-		la.nleaves = nleaves;
-		la.pc = o.pc;
-		la.pc_list = o.pc_list;
-		la.pp = o.pp;
-		la.pp_list = o.pp_list;
-		for (int d = 0; d < 3; d++) {
-			la.x[d] = b->x[d];
-			la.v[d] = b->v[d];
-			la.g[d] = b->g[d];
-		}
-		la.rung = b->rung;
-		la.pot = b->pot;
-		la.kp = *kp;
-		la.compensated = c->compensated;
-		la.sums = counters + 4;
-		la.max_rung = c->d_flags + 48;
-		const bool fused = getenv("CT_LEAF_FUSED") != nullptr && b->nsub == 1 && !b->d_sub_h;
-		if (fused) {
-			cudaEventRecord(c->ev[4], st);
-			if (nleaves > 0) {
-				c->launches++;
-				k_leaf<Ops><<<(int) std::min<int64_t>(nleaves, (int64_t) c->nsm * 16), LEAF_TPB, 0, st>>>(la);
-			}
-			cudaEventRecord(c->ev[5], st);
-		} else if (nleaves > 0) {
+		cudaEventRecord(c->ev[4], st);
+		cudaEventRecord(c->ev[5], st);
+		cudaEventRecord(c->ev[12], st);  // no leaves: zero P2P and leaf-kick times
+		if (nleaves > 0) {
 			// 32-sink tiles of the leaves
 			ct_status s2 = CT_OK;
 			int* ntl = (int*) scratch(c, 40, sizeof(int) * (nleaves + 1), &s2);
@@ -1848,8 +1562,8 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		C.ms_walk = elapsed_ms(c->ev[0], c->ev[1]);
 		C.ms_m2l = elapsed_ms(c->ev[1], c->ev[2]);
 		C.ms_l2l = elapsed_ms(c->ev[2], c->ev[3]);
-		C.ms_leaf = elapsed_ms(c->ev[4], c->ev[5]);  // the P2P kernel (or the fused leaf kernel)
-		if (!fused && nleaves > 0) {
+		C.ms_leaf = elapsed_ms(c->ev[4], c->ev[5]);  // the P2P kernels
+		if (nleaves > 0) {
 			C.ms_leafkick = elapsed_ms(c->ev[5], c->ev[12]);
 		}
 		b->have_force = kp->save_force != 0;
