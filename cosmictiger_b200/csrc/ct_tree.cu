@@ -450,16 +450,17 @@ __device__ __forceinline__ T warp_sum(T v) {
 
 constexpr int UTPB = 128;
 
+// A warp per node (tree.cpp:351-571): tight box, expansion centre and radius, multipole (P2M of
+// the particles for a leaf, M2M of the two children in double for an interior node).
 template<class Ops>
 __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW* nodes, int32_t* nbox, float* multi, double* tbox, const double* gbox,
 		const uint32_t* x0, const uint32_t* x1, const uint32_t* x2, int bucket) {
 	constexpr int NM = Ops::NMULT;
-	__shared__ double sd[UTPB / 32][NM + 8];
-	__shared__ double s_X[3];
-	__shared__ float s_r2;
 	const uint32_t* xs[3] = { x0, x1, x2 };
-	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-	for (int64_t ni = lb + blockIdx.x; ni < le; ni += gridDim.x) {
+	const int lane = threadIdx.x & 31;
+	const int64_t gw = (blockIdx.x * (int64_t) blockDim.x + threadIdx.x) >> 5;
+	const int64_t nw = ((int64_t) gridDim.x * blockDim.x) >> 5;
+	for (int64_t ni = lb + gw; ni < le; ni += nw) {
 		const NodeW nd = nodes[ni];
 		const int nparts = nd.pend - nd.pbeg;
 		const double* gb = gbox + 6 * ni;
@@ -470,7 +471,7 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 				mn[d] = gb[3 + d];
 				mx[d] = gb[d];
 			}
-			for (int p = nd.pbeg + threadIdx.x; p < nd.pend; p += UTPB) {
+			for (int p = nd.pbeg + lane; p < nd.pend; p += 32) {
 				for (int d = 0; d < 3; d++) {
 					const double xx = fixed_to_double(xs[d][p]);
 					mx[d] = fmax(mx[d], xx);
@@ -481,26 +482,12 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 				mn[d] = warp_min(mn[d]);
 				mx[d] = warp_max(mx[d]);
 			}
-			if (lane == 0) {
-				for (int d = 0; d < 3; d++) {
-					sd[w][d] = mn[d];
-					sd[w][3 + d] = mx[d];
-				}
-			}
-			__syncthreads();
-			for (int d = 0; d < 3; d++) {
-				for (int k = 0; k < UTPB / 32; k++) {
-					mn[d] = fmin(mn[d], sd[k][d]);
-					mx[d] = fmax(mx[d], sd[k][3 + d]);
-				}
-			}
-			__syncthreads();
 			double Xc[3];
 			for (int d = 0; d < 3; d++) {
 				Xc[d] = (mx[d] + mn[d]) * 0.5;
 			}
 			double r = 0.0;
-			for (int p = nd.pbeg + threadIdx.x; p < nd.pend; p += UTPB) {
+			for (int p = nd.pbeg + lane; p < nd.pend; p += 32) {
 				double this_radius = 0.0;
 				for (int d = 0; d < 3; d++) {
 					const double dx = fixed_to_double(xs[d][p]) - Xc[d];
@@ -518,7 +505,7 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 			for (int k = 0; k < NM; k++) {
 				M[k] = 0.0;
 			}
-			for (int p = nd.pbeg + threadIdx.x; p < nd.pend; p += UTPB) {
+			for (int p = nd.pbeg + lane; p < nd.pend; p += 32) {
 				float m[NM];
 				Ops::p2m(m, fixed_dist(x0[p], Y[0]), fixed_dist(x1[p], Y[1]), fixed_dist(x2[p], Y[2]));
 				for (int k = 0; k < NM; k++) {
@@ -529,22 +516,11 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 				M[k] = warp_sum(M[k]);
 			}
 			if (lane == 0) {
-				for (int k = 0; k < NM; k++) {
-					sd[w][k] = M[k];
-				}
-				sd[w][NM] = r;
-			}
-			__syncthreads();
-			if (threadIdx.x == 0) {
-				double rr = 0.0;
-				for (int k = 0; k < UTPB / 32; k++) {
-					rr = fmax(rr, sd[k][NM]);
-				}
 				NodeW o = nd;
 				o.x = Y[0];
 				o.y = Y[1];
 				o.z = Y[2];
-				o.radius = (float) sqrt(rr);
+				o.radius = (float) sqrt(r);
 				nodes[ni] = o;
 				for (int d = 0; d < 3; d++) {
 					tbox[6 * ni + d] = mn[d];
@@ -553,14 +529,12 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 					nbox[6 * ni + 3 + d] = range_fixed_from_double(mx[d]);
 				}
 			}
-			for (int k = threadIdx.x; k < NM; k += UTPB) {
-				double s = 0.0;
-				for (int q = 0; q < UTPB / 32; q++) {
-					s += sd[q][k];
+#pragma unroll
+			for (int k = 0; k < NM; k++) {
+				if (lane == (k & 31)) {
+					multi[NMULT_STRIDE * ni + k] = (float) M[k];
 				}
-				multi[NMULT_STRIDE * ni + k] = (float) s;
 			}
-			__syncthreads();
 		} else {
 			// ---- interior node (tree.cpp:351-497)
 			const int64_t L = nd.child, R = nd.child + 1;
@@ -594,14 +568,14 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 			}
 			const bool tried1 = nparts <= 64 * bucket && (be[xdim] - bb[xdim] <= 0.5);
 			double Xc1[3];
+			float r2max = 0.0f;
 			if (tried1) {
 				uint32_t xc[3];
 				for (int d = 0; d < 3; d++) {
 					Xc1[d] = 0.5 * (bb[d] + be[d]);
 					xc[d] = fixed_from_double(Xc1[d]);
 				}
-				float r2max = 0.0f;
-				for (int p = nd.pbeg + threadIdx.x; p < nd.pend; p += UTPB) {
+				for (int p = nd.pbeg + lane; p < nd.pend; p += 32) {
 					const float dx = fixed_dist(x0[p], xc[0]);
 					const float dy = fixed_dist(x1[p], xc[1]);
 					const float dz = fixed_dist(x2[p], xc[2]);
@@ -609,23 +583,12 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 					r2max = fmaxf(r2max, r2);
 				}
 				r2max = warp_max(r2max);
-				if (lane == 0) {
-					sd[w][0] = r2max;
-				}
-				__syncthreads();
-				if (threadIdx.x == 0) {
-					float m = 0.f;
-					for (int k = 0; k < UTPB / 32; k++) {
-						m = fmaxf(m, (float) sd[k][0]);
-					}
-					s_r2 = m;
-				}
-				__syncthreads();
 			}
-			if (threadIdx.x == 0) {
+			double sX[3];
+			{
 				const double Xl[3] = { fixed_to_double(nl.x), fixed_to_double(nl.y), fixed_to_double(nl.z) };
 				const double Xr[3] = { fixed_to_double(nr.x), fixed_to_double(nr.y), fixed_to_double(nr.z) };
-				const double radius1 = tried1 ? (double) sqrtf(s_r2) : 0.0;
+				const double radius1 = tried1 ? (double) sqrtf(r2max) : 0.0;
 				double N[3];
 				double norminv = 0.0;
 				for (int d = 0; d < 3; d++) {
@@ -689,41 +652,44 @@ __global__ void __launch_bounds__(UTPB) k_upsweep(int64_t lb, int64_t le, NodeW*
 					}
 				}
 				for (int d = 0; d < 3; d++) {
-					s_X[d] = Xc[d];
+					sX[d] = Xc[d];
 				}
 				NodeW o = nd;
 				o.x = fixed_from_double(Xc[0]);
 				o.y = fixed_from_double(Xc[1]);
 				o.z = fixed_from_double(Xc[2]);
 				o.radius = radius;
-				nodes[ni] = o;
-				for (int d = 0; d < 3; d++) {
-					tbox[6 * ni + d] = bb[d];
-					tbox[6 * ni + 3 + d] = be[d];
-					nbox[6 * ni + d] = range_fixed_from_double(bb[d]);
-					nbox[6 * ni + 3 + d] = range_fixed_from_double(be[d]);
+				if (lane == 0) {
+					nodes[ni] = o;
+					for (int d = 0; d < 3; d++) {
+						tbox[6 * ni + d] = bb[d];
+						tbox[6 * ni + 3 + d] = be[d];
+						nbox[6 * ni + d] = range_fixed_from_double(bb[d]);
+						nbox[6 * ni + 3 + d] = range_fixed_from_double(be[d]);
+					}
 				}
 			}
-			__syncthreads();
-			// M2M of both children in double (tree.cpp:481-494): thread 0 left, thread 32 right
-			if (threadIdx.x == 0 || threadIdx.x == 32) {
-				const bool left = threadIdx.x == 0;
-				const int64_t c = left ? L : R;
-				const NodeW cn = left ? nl : nr;
-				double Ma[NM], Mo[NM];
+			// M2M of both children in double (tree.cpp:481-494): lane 0 the left, lane 1 the right,
+			// then left + right
+			double Mo[NM];
+			for (int k = 0; k < NM; k++) {
+				Mo[k] = 0.0;
+			}
+			if (lane < 2) {
+				const int64_t c = lane == 0 ? L : R;
+				const NodeW cn = lane == 0 ? nl : nr;
+				double Ma[NM];
 				for (int k = 0; k < NM; k++) {
 					Ma[k] = (double) multi[NMULT_STRIDE * c + k];
 				}
-				Ops::m2m(Mo, Ma, fixed_to_double(cn.x) - s_X[0], fixed_to_double(cn.y) - s_X[1], fixed_to_double(cn.z) - s_X[2]);
-				for (int k = 0; k < NM; k++) {
-					sd[left ? 0 : 1][k] = Mo[k];
+				Ops::m2m(Mo, Ma, fixed_to_double(cn.x) - sX[0], fixed_to_double(cn.y) - sX[1], fixed_to_double(cn.z) - sX[2]);
+			}
+			for (int k = 0; k < NM; k++) {
+				const double right = __shfl_down_sync(0xffffffffu, Mo[k], 1);
+				if (lane == 0) {
+					multi[NMULT_STRIDE * ni + k] = (float) (Mo[k] + right);
 				}
 			}
-			__syncthreads();
-			for (int k = threadIdx.x; k < NM; k += UTPB) {
-				multi[NMULT_STRIDE * ni + k] = (float) (sd[0][k] + sd[1][k]);
-			}
-			__syncthreads();
 		}
 	}
 }
@@ -877,7 +843,8 @@ ct_status tree_build_t(Ctx* c, Box* b, const ct_tree_params* p) {
 		const int64_t a = levels[k], e = levels[k + 1];
 		if (e > a) {
 			c->launches++;
-			k_upsweep<Ops><<<(int) std::min<int64_t>(e - a, (int64_t) c->nsm * 32), UTPB, 0, st>>>(a, e, b->nodes, b->nbox, b->multi, b->tbox, b->gbox,
+			k_upsweep<Ops><<<(int) std::min<int64_t>((e - a + UTPB / 32 - 1) / (UTPB / 32), (int64_t) c->nsm * 16), UTPB, 0, st>>>(a, e, b->nodes, b->nbox,
+					b->multi, b->tbox, b->gbox,
 					b->x[0], b->x[1], b->x[2], p->bucket);
 		}
 	}
