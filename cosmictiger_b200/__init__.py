@@ -145,6 +145,8 @@ def library():
     L.ct_sort_by_rung.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
     L.ct_ctx_set_compensated.argtypes = [vp, i32]
     L.ct_ensemble_reshape.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
+    L.ct_box_get_rung_state.argtypes = [vp, i32, ctypes.POINTER(i64), vp, ctypes.POINTER(i32)]
+    L.ct_box_set_rung_state.argtypes = [vp, i32, i64, vp, i32]
     L.ct_tree_create.argtypes = [vp, i32, ctypes.POINTER(TreeParams), ctypes.POINTER(i64)]
     L.ct_kick.argtypes = [vp, i32, ctypes.POINTER(KickParams), ctypes.POINTER(KickReturn)]
     L.ct_drift.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_double]
@@ -258,6 +260,19 @@ class Box:
         self.counts = c
         self.n = int(np.sum(c))
         self.tree_params = None
+
+    def rung_state(self):
+        """(active range start, saved starts of the enclosing ranges) of the rung ladder."""
+        rb = ctypes.c_int64()
+        depth = ctypes.c_int(0)
+        self.ctx.check(self.ctx.lib.ct_box_get_rung_state(self.ctx.h, self.id, ctypes.byref(rb), None, ctypes.byref(depth)), "ct_box_get_rung_state")
+        stack = np.zeros(max(depth.value, 1), np.int64)
+        self.ctx.check(self.ctx.lib.ct_box_get_rung_state(self.ctx.h, self.id, ctypes.byref(rb), _p(stack), ctypes.byref(depth)), "ct_box_get_rung_state")
+        return int(rb.value), [int(q) for q in stack[:depth.value]]
+
+    def set_rung_state(self, rung_begin, stack):
+        s = np.ascontiguousarray(stack if len(stack) else [0], np.int64)
+        self.ctx.check(self.ctx.lib.ct_box_set_rung_state(self.ctx.h, self.id, int(rung_begin), _p(s), len(stack)), "ct_box_set_rung_state")
 
     def set_first_call(self, flags):
         f = np.ascontiguousarray(flags, np.int32)

@@ -190,6 +190,47 @@ extern "C" ct_status ct_rung_counts(ct_ctx* ctx, int box_id, uint64_t* counts) {
 	return rung_counts(c, c->boxes[box_id], counts);
 }
 
+extern "C" ct_status ct_box_get_rung_state(ct_ctx* ctx, int box_id, int64_t* rung_begin, int64_t* stack, int* depth) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c || box_id < 0 || box_id >= (int) c->boxes.size() || !c->boxes[box_id] || !depth) {
+		return fail(c, CT_ERR_ARG, "ct_box_get_rung_state: bad arguments");
+	}
+	const Box* b = c->boxes[box_id];
+	if (rung_begin) {
+		*rung_begin = b->rung_begin;
+	}
+	if (stack) {
+		if (*depth < (int) b->rung_stack.size()) {
+			return fail(c, CT_ERR_ARG, "ct_box_get_rung_state: stack buffer too small");
+		}
+		for (size_t i = 0; i < b->rung_stack.size(); i++) {
+			stack[i] = b->rung_stack[i];
+		}
+	}
+	*depth = (int) b->rung_stack.size();
+	return CT_OK;
+}
+
+extern "C" ct_status ct_box_set_rung_state(ct_ctx* ctx, int box_id, int64_t rung_begin, const int64_t* stack, int depth) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c || box_id < 0 || box_id >= (int) c->boxes.size() || !c->boxes[box_id] || depth < 0 || (depth > 0 && !stack)) {
+		return fail(c, CT_ERR_ARG, "ct_box_set_rung_state: bad arguments");
+	}
+	Box* b = c->boxes[box_id];
+	if (rung_begin < 0 || rung_begin > b->n) {
+		return fail(c, CT_ERR_ARG, "ct_box_set_rung_state: active range start outside the box");
+	}
+	for (int i = 0; i < depth; i++) {
+		if (stack[i] < 0 || stack[i] > b->n) {
+			return fail(c, CT_ERR_ARG, "ct_box_set_rung_state: saved range start outside the box");
+		}
+	}
+	b->rung_begin = rung_begin;
+	b->rung_stack.assign(stack, stack + depth);
+	b->tree_valid = false;
+	return CT_OK;
+}
+
 extern "C" ct_status ct_step_hierarchical(ct_ctx* ctx, int box_id, const ct_step_params* params, ct_step_return* result) {
 	Ctx* c = (Ctx*) ctx;
 	if (!c || box_id < 0 || box_id >= (int) c->boxes.size() || !c->boxes[box_id] || !params) {

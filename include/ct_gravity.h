@@ -200,6 +200,13 @@ typedef struct {
 } ct_step_return;
 
 ct_status ct_step_hierarchical(ct_ctx* ctx, int box_id, const ct_step_params* params, ct_step_return* result);
+/* The active-range state of the hierarchical rung ladder: the start of the active range
+ * (particles_current_range) and the saved starts of the enclosing ranges, innermost last
+ * (particles_push/pop_rungs, src/particles.cpp:218-235) -- what particles_save writes after
+ * the particles (src/particles.cpp:1216-1219), so that a run resumes where it stopped.
+ * get: pass stack = NULL to learn the depth; set: restores both (begin <= box size). */
+ct_status ct_box_get_rung_state(ct_ctx* ctx, int box_id, int64_t* rung_begin, int64_t* stack, int* depth);
+ct_status ct_box_set_rung_state(ct_ctx* ctx, int box_id, int64_t rung_begin, const int64_t* stack, int depth);
 /* Particle counts per rung 0..15 (particles_rung_counts, src/particles.cpp:583). */
 ct_status ct_rung_counts(ct_ctx* ctx, int box_id, uint64_t* counts);
 

@@ -1,0 +1,101 @@
+"""The reference's checkpoint layout (write_checkpoint, src/driver.cpp:1143-1173; particles_save,
+src/particles.cpp:1206-1227; domains_save, src/domain.cpp:87-94): struct sizes and offsets,
+byte-level layout of the particle section, round trips, and resuming a hierarchical run from a
+checkpoint on the device."""
+import struct
+
+import numpy as np
+import pytest
+
+from cosmictiger_b200 import checkpoint as ck
+
+
+def test_struct_layouts():
+    d = ck.DRIVER_PARAMS
+    assert d.itemsize == 176
+    assert d.fields["energies"][1] == 48 and d.fields["max_rung"][1] == 112 and d.fields["bucket_size"][1] == 128
+    assert d.fields["total_processed"][1] == 136 and d.fields["flops"][1] == 144 and d.fields["itime"][1] == 168
+    assert ck.DOMAIN_ENTRY.itemsize == 72  # pair<size_t, domain_t>: 8 + (48 + 8 + 4 + 4)
+    assert ck.domain_local_dtype(False).itemsize == 72 and ck.domain_local_dtype(True).itemsize == 80
+
+
+def test_particle_section_bytes(tmp_path):
+    """The bytes after driver_params follow particles_save field by field."""
+    x = np.array([1, 2, 3], np.uint32)
+    y = np.array([4, 5, 6], np.uint32)
+    z = np.array([7, 8, 2 ** 32 - 1], np.uint32)
+    v = np.arange(9, dtype=np.float32).reshape(3, 3)
+    r = np.array([0, 2, 1], np.int8)
+    p = tmp_path / "c.dat"
+    ck.write_checkpoint(str(p), ck.default_params(a=0.5, iter=7), x, y, z, v, r, rung_begin=1, rung_begins=[0])
+    raw = p.read_bytes()
+    body = raw[176:]
+    want = struct.pack("<i", 3) + struct.pack("<3I", 1, 2, 3) + struct.pack("<3I", 4, 5, 6) + struct.pack("<3I", 7, 8, 2 ** 32 - 1)
+    want += struct.pack("<9f", *range(9)) + struct.pack("<3b", 0, 2, 1) + struct.pack("<3i", 1, 1, 0)
+    assert body[:len(want)] == want
+    # domains: one entry (key 1, unit box, midx 0.5, rank 0) and one domain_local
+    dom = body[len(want):]
+    assert len(dom) == 8 + 72 + 72
+    assert struct.unpack("<Q", dom[:8])[0] == 1
+    params = np.frombuffer(raw[:176], ck.DRIVER_PARAMS)[0]
+    assert params["a"] == 0.5 and params["iter"] == 7
+
+
+def test_round_trip_and_truncation(tmp_path):
+    rng = np.random.default_rng(3)
+    n = 1000
+    x, y, z = (rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32) for _ in range(3))
+    v = rng.standard_normal((n, 3)).astype(np.float32)
+    r = rng.integers(0, 5, n).astype(np.int8)
+    p = tmp_path / "c.dat"
+    params = ck.default_params(a=1.0, tau=0.25, max_rung=4, minrung0=1, step=3, bucket_size=128)
+    ck.write_checkpoint(str(p), params, x, y, z, v, r, rung_begin=700, rung_begins=[0, 300, 600])
+    c = ck.read_checkpoint(str(p))
+    for k, a in (("x", x), ("y", y), ("z", z), ("v", v), ("rung", r)):
+        assert np.array_equal(c[k], a), k
+    assert c["rung_begin"] == 700 and c["rung_begins"] == [0, 300, 600]
+    assert c["params"]["max_rung"] == 4 and c["params"]["tau"] == 0.25
+    assert c["domain_local"]["part_range"][0].tolist() == [0, n]
+    raw = p.read_bytes()
+    (tmp_path / "t.dat").write_bytes(raw[:-5])
+    with pytest.raises(ck.CheckpointError):
+        ck.read_checkpoint(str(tmp_path / "t.dat"))
+    with pytest.raises(ck.CheckpointError):
+        ck.read_checkpoint(str(p), lightcone=True)
+
+
+@pytest.mark.gpu
+def test_resume_hierarchical_run_from_checkpoint(tmp_path):
+    """Two hierarchical steps, checkpoint, two more, against the same four steps with a reload
+    from the checkpoint in between: bit-identical particles and rung-ladder state."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import ics
+
+    x, y, z, v, r = ics.clustered_box(16, nspheres=20, seed=41)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    ctx = ct.Context(order=7)
+
+    def run(box, steps, state):
+        for _ in range(steps):
+            sp = ct.StepParams(minrung=state["minrung"], minrung0=0, max_rung=state["max_rung"], a=1.0, tau=state["tau"], t0=0.01, theta=0.55, hsoft=h,
+                               bucket=128, eta=ics.eta_default(), GM=1.0 / N, max_dt=1e30, do_phi=1, nocrop=1, drag=0.0, sign=1.0)
+            res = box.step_hierarchical(sp)
+            state.update(minrung=res.minrung, max_rung=res.max_rung, tau=state["tau"] + 0.01)
+
+    a = ctx.box(N)
+    a.upload(x, y, z, v, r)
+    sa = {"minrung": 0, "max_rung": 0, "tau": 0.0}
+    run(a, 2, sa)
+    path = str(tmp_path / "ck.dat")
+    ck.save_box(path, a, ck.default_params(a=1.0, tau=sa["tau"], max_rung=sa["max_rung"], minrung0=sa["minrung"], step=2, bucket_size=128))
+    run(a, 2, sa)
+    b, params = ck.load_box(ctx, path)
+    sb = {"minrung": int(params["minrung0"]), "max_rung": int(params["max_rung"]), "tau": float(params["tau"])}
+    run(b, 2, sb)
+    oa, ob = a.download(), b.download()
+    for f in ("x", "y", "z", "v", "rung"):
+        assert np.array_equal(oa[f], ob[f]), f
+    assert a.rung_state() == b.rung_state()
+    assert sa == sb
+    ctx.close()
