@@ -346,27 +346,31 @@ def main():
     e2e = None
     if not args.no_e2e:
         cur = box.download()
-        hx, hy, hz = (torch.from_numpy(cur[k].view(np.int32).copy()).pin_memory().numpy().view(np.uint32) for k in ("x", "y", "z"))
-        hv = torch.from_numpy(cur["v"].copy()).pin_memory().numpy()
-        hr = torch.from_numpy(cur["rung"].copy()).pin_memory().numpy()
-        ox, oy, oz = (torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32) for _ in range(3))
-        ov = torch.empty((N, 3), dtype=torch.float32).pin_memory().numpy()
-        orr = torch.empty(N, dtype=torch.int8).pin_memory().numpy()
+        def pinned_set(src=None):
+            xyz = [torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32) for _ in range(3)]
+            vv = torch.empty((N, 3), dtype=torch.float32).pin_memory().numpy()
+            rr = torch.empty(N, dtype=torch.int8).pin_memory().numpy()
+            if src is not None:
+                for a, k in zip(xyz, ("x", "y", "z")):
+                    np.copyto(a, src[k])
+                np.copyto(vv, src["v"])
+                np.copyto(rr, src["rung"])
+            return xyz + [vv, rr]
+
+        # two pinned host sets used in turn: each step uploads the particles from one and
+        # downloads its result into the other, which the next step uploads
+        bufs = [pinned_set(cur), pinned_set()]
 
         def e2e_step(first):
-            box.upload(hx, hy, hz, hv, hr)
+            src, dst = bufs[0], bufs[1]
+            box.upload(*src)
             if ms is not None:
                 mstep()
             else:
                 step(first)
             p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
-            ctx.check(ctx.lib.ct_box_download(ctx.h, box.id, p(ox), p(oy), p(oz), p(ov), p(orr), None, None, None, None), "download")
-            # the next step starts from this step's result
-            np.copyto(hx, ox)
-            np.copyto(hy, oy)
-            np.copyto(hz, oz)
-            np.copyto(hv, ov)
-            np.copyto(hr, orr)
+            ctx.check(ctx.lib.ct_box_download(ctx.h, box.id, *[p(a) for a in dst], None, None, None, None), "download")
+            bufs.reverse()
 
         e2e_step(True)
         torch.cuda.synchronize()
