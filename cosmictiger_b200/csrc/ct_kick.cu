@@ -490,9 +490,10 @@ __global__ void __launch_bounds__(128, 3) k_m2l_ewald(int64_t nn, const NodeW* _
 
 // Direct M2L: dL += sum over the direct CC list.
 template<class Ops>
-__global__ void __launch_bounds__(128) k_m2l_direct(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi,
+__global__ void __launch_bounds__(128, 3) k_m2l_direct(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi,
 		const int2* __restrict__ dcc, const int* __restrict__ dcc_list, float* __restrict__ dL, int do_phi) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
+	__shared__ float s_L[4][32][51];
 	const int lane = threadIdx.x & 31;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -502,7 +503,8 @@ __global__ void __launch_bounds__(128) k_m2l_direct(int64_t nn, const NodeW* __r
 			continue;
 		}
 		const NodeW self = nodes[si];
-		float L[NE];
+		// this lane's expansion sum in shared memory (rows of 51 floats: lanes on distinct banks)
+		float* L = &s_L[threadIdx.x >> 5][lane][0];
 		for (int i = 0; i < NE; i++) {
 			L[i] = 0.f;
 		}
@@ -522,12 +524,16 @@ __global__ void __launch_bounds__(128) k_m2l_direct(int64_t nn, const NodeW* __r
 			Ops::greens(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z));
 			Ops::m2l(L, M, D, do_phi != 0);
 		}
-		warp_reduce_arr<NE>(L);
-		if (lane == 0) {
-			for (int i = 0; i < NE; i++) {
-				dL[NEXP_STRIDE * si + i] += L[i];
+		__syncwarp();
+		// entry n summed over the 32 lanes' rows by lane n % 32
+		for (int n = lane; n < NE; n += 32) {
+			float t = 0.f;
+			for (int q = 0; q < 32; q++) {
+				t += s_L[threadIdx.x >> 5][q][n];
 			}
+			dL[NEXP_STRIDE * si + n] += t;
 		}
+		__syncwarp();
 	}
 }
 
