@@ -535,6 +535,7 @@ void ct_ctx_destroy(ct_ctx* ctx) {
 			ct_box_destroy(ctx, (int) i);
 		}
 	}
+	kick_buffers_release(c);
 	for (auto& s : c->scratch) {
 		dfree(c, s.p, s.bytes);
 	}

@@ -118,6 +118,8 @@ struct Box {
 	bool have_force = false;
 };
 
+struct KickBuffers;  // interaction lists and expansions of the kick (ct_kick.cu)
+
 // Host-visible error state and stream.
 struct Ctx {
 	int device = 0;
@@ -141,6 +143,7 @@ struct Ctx {
 	bool drift_timed = false;         // ev[6], ev[7] hold a recorded drift
 	unsigned long long launches = 0;  // kernels of this library launched so far
 	int compensated = 1;              // Neumaier-compensated P2P batch sums
+	KickBuffers* kick = nullptr;      // owned; grown by the kick, freed with the context
 };
 
 // Device time between two recorded events, 0 if it is not available.  A failed query sets the
@@ -154,6 +157,9 @@ inline float elapsed_ms(cudaEvent_t a, cudaEvent_t b) {
 	}
 	return ms;
 }
+
+// Frees the context's kick buffers (called by ct_ctx_destroy).
+void kick_buffers_release(Ctx* c);
 
 // Allocation with budget accounting.
 ct_status dalloc(Ctx* c, void** p, size_t bytes, const char* what);

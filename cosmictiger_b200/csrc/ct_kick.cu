@@ -1268,6 +1268,8 @@ __global__ void k_collect_leaves(int64_t nn, const NodeW* nodes, int64_t* leaves
 }
 
 // ---------------------------------------------------------------- host driver
+}  // namespace
+
 struct KickBuffers {
 	int2* per_node = nullptr;  // 7 arrays of nnodes
 	size_t per_node_n = 0;
@@ -1292,16 +1294,14 @@ struct KickBuffers {
 	size_t leaves_n = 0;
 };
 
-std::vector<std::pair<Ctx*, KickBuffers>> g_kb;
+namespace {
+
 
 KickBuffers& kbuf(Ctx* c) {
-	for (auto& e : g_kb) {
-		if (e.first == c) {
-			return e.second;
-		}
+	if (!c->kick) {
+		c->kick = new KickBuffers();
 	}
-	g_kb.emplace_back(c, KickBuffers());
-	return g_kb.back().second;
+	return *c->kick;
 }
 
 template<class T>
@@ -1606,6 +1606,23 @@ ct_status ewald_init(Ctx* c) {
 		dfree(c, d, sizeof(h));
 	}
 	return CT_OK;
+}
+
+void kick_buffers_release(Ctx* c) {
+	KickBuffers* K = c->kick;
+	if (!K) {
+		return;
+	}
+	dfree(c, K->per_node, sizeof(int2) * K->per_node_n);
+	dfree(c, K->cc, sizeof(int) * K->cc_n);
+	dfree(c, K->leafl, sizeof(int) * K->leaf_n);
+	dfree(c, K->pass, sizeof(int) * K->pass_n);
+	dfree(c, K->stage, sizeof(int) * K->stage_n);
+	dfree(c, K->dL, sizeof(float) * K->dL_n);
+	dfree(c, K->Lx, sizeof(float) * K->Lx_n);
+	dfree(c, K->leaves, sizeof(int64_t) * K->leaves_n);
+	delete K;
+	c->kick = nullptr;
 }
 
 ct_status kick_run(Ctx* c, Box* b, const ct_kick_params* p, ct_kick_return* out) {

@@ -65,6 +65,33 @@ def test_counters_before_any_drift_leave_no_stale_error():
     c.close()
 
 
+def test_context_destroy_frees_device_memory():
+    """A context's device memory (boxes, trees, kick lists, scratch) is returned when the
+    context is destroyed, however many contexts come and go."""
+    import torch
+
+    import cosmictiger_b200 as ct
+
+    torch.cuda.init()
+    x, y, z, v, r = lattice(24, seed=9)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    free0 = None
+    for rep in range(3):
+        c = ct.Context(order=7)
+        b = c.box(N)
+        b.upload(x, y, z, v, r)
+        b.tree_create(0.55, h, 128)
+        b.kick(kick_params(0.55, h, N))
+        assert c.bytes_in_use() > 0
+        c.close()
+        torch.cuda.synchronize()
+        free = torch.cuda.mem_get_info()[0]
+        if free0 is None:
+            free0 = free
+        assert abs(free - free0) < (32 << 20), (rep, free0, free)
+
+
 def test_drift_bitexact(ctx, oracle):
     rng = np.random.default_rng(7)
     N = 50000
