@@ -56,10 +56,11 @@ def parse():
     ap.add_argument("--ensemble-nmin", type=int, default=16)
     ap.add_argument("--ensemble-nmax", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=3)
-    ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving"],
+    ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving", "lightcone"],
                     help="instead of the benchmark line: precision (theta x order x summation, force error vs FP64 Ewald and "
                          "particle-steps/s), ensemble (512 boxes of 16^3..128^3, batched vs box by box, 20 steps) or serving "
-                         "(Poisson arrivals of 32^3..256^3 requests, rate sweep, p50/p99 latency vs sequential runs)")
+                         "(Poisson arrivals of 32^3..256^3 requests, rate sweep, p50/p99 latency vs sequential runs) or lightcone "
+                         "(drift with the lightcone capture vs plain drift)")
     ap.add_argument("--study-seed", type=int, default=11)
     return ap.parse_args()
 
@@ -707,11 +708,86 @@ def study_serving(args, torch):
     return {"study": "serving", "n_range": [32, 256], "steps_range": [1, 16], "hbm_budget_gb": 150, "rows": out}
 
 
+def study_lightcone(args, torch):
+    """Drift with the lightcone capture (cuda_drift with do_lc) on the benchmark box, every
+    particle on rung 0: plain drift vs drift + capture per call (CUDA events on the library's
+    stream; the capture's call includes its read-back of the entry count), entries per drift,
+    and the HBM rate of the capture against the measured copy bandwidth (algorithmic bytes:
+    37 per particle (positions and velocities read, rung read, positions written) + 28 per
+    entry).  The observer's cone sweeps a shell at distance about tau_max - tau (tau_max 1.6,
+    drifts of dt 0.005 from tau 0.7, so the shell sits near radius 0.9)."""
+    import cosmictiger_b200 as ct
+    from tests import oracle_lib
+
+    state = make_ics(args, seed=args.study_seed)
+    x, y, z, v, _ = state
+    N = len(x)
+    r0 = np.zeros(N, np.int8)
+    ctx = ct.Context(order=7)
+    lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
+    box = ctx.box(N)
+    box.upload(x, y, z, v, r0)
+    dt, tau_max, K = 0.005, 1.6, 10
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        ms = []
+        for i in range(3 + K):
+            ctx.synchronize()
+            e0.record(lib_stream)
+            fn(i)
+            e1.record(lib_stream)
+            ctx.synchronize()
+            torch.cuda.synchronize()
+            if i >= 3:
+                ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    ms_plain = timed(lambda i: box.drift(0, 1.0, dt))
+    rows = []
+    hbm = peaks_hbm()
+    for nside in (64, 4096):
+        counts = []
+
+        def lc(i):
+            tau0 = 0.7 + dt * i
+            counts.append(box.drift_lightcone(0, 1.0, dt, tau0, tau0 + dt, tau_max, nside))
+
+        ms = timed(lc)
+        box.lightcone(clear=True)
+        ent = float(np.mean(counts[3:]))
+        gbs = (37.0 * N + 28.0 * ent) / (ms / 1e3) / 1e9
+        rows.append({"nside": nside, "ms_per_drift": ms, "entries_per_drift": ent, "particles_s": N / (ms / 1e3), "achieved_gbs": gbs,
+                     "hbm_peak_gbs": hbm, "frac": gbs / hbm if hbm else None})
+        print(json.dumps(rows[-1]), flush=True)
+    box.close()
+    ctx.close()
+    # the CPU oracle (one thread) on the first 2^20 particles
+    O = oracle_lib.load(build=False)
+    m = min(N, 1 << 20)
+    xs, ys, zs, vs = (np.ascontiguousarray(q[:m]).copy() for q in (x, y, z, v))
+    t = time.perf_counter()
+    ent = O.drift_lc(xs, ys, zs, vs, r0[:m].copy(), 0, 1.0, dt, 0.7, 0.7 + dt, tau_max, 64)
+    cpu_s = time.perf_counter() - t
+    return {"study": "lightcone", "workload": workload_name(args).replace("4-rung hierarchical steps", "drift of every particle") + ", seed %d" % args.study_seed,
+            "particles": N, "dt": dt, "tau_max": tau_max, "plain_drift_ms": ms_plain, "plain_particles_s": N / (ms_plain / 1e3), "rows": rows,
+            "cpu_baseline": {"value": m / cpu_s, "unit": "particles/s", "cores": 1, "kind": "port", "sample": "%d particles, %d entries" % (m, len(ent))}}
+
+
+def peaks_hbm():
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def run_study(args):
     import torch
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    fn = {"precision": study_precision, "ensemble": study_ensemble, "serving": study_serving}[args.study]
+    fn = {"precision": study_precision, "ensemble": study_ensemble, "serving": study_serving, "lightcone": study_lightcone}[args.study]
     t = time.perf_counter()
     res = fn(args, torch)
     res["wall_s"] = time.perf_counter() - t

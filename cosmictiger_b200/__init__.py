@@ -117,6 +117,15 @@ NODE_DTYPE = np.dtype(
     align=True,
 )
 
+# one lightcone crossing (ct_lc_entry; the reference's lc_entry, cosmictiger/lightcone.hpp:54-58):
+# position fixed<int,31> relative to the observer, velocity after drag, HEALPix nested pixel
+LC_ENTRY = np.dtype([("x", "<i4"), ("y", "<i4"), ("z", "<i4"), ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4"), ("pix", "<i4")])
+
+
+class LcParams(ctypes.Structure):
+    _fields_ = [("tau0", ctypes.c_float), ("tau1", ctypes.c_float), ("tau_max", ctypes.c_float), ("nside", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -167,6 +176,10 @@ def library():
     L.ct_launch_count.argtypes = [vp]
     L.ct_launch_count.restype = ctypes.c_ulonglong
     L.ct_direct_ewald.argtypes = [vp, i32, i64, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
+    L.ct_drift_lightcone.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_double, ctypes.POINTER(LcParams), ctypes.POINTER(i64)]
+    L.ct_lightcone_count.argtypes = [vp, i32, ctypes.POINTER(i64)]
+    L.ct_lightcone_download.argtypes = [vp, i32, vp, i64, ctypes.POINTER(i64), i32]
+    L.ct_lightcone_reserve.argtypes = [vp, i32, i64]
     _lib = L
     return L
 
@@ -349,6 +362,24 @@ class Box:
 
     def drift(self, rung, a, dt, drag=0.0):
         self.ctx.check(self.ctx.lib.ct_drift(self.ctx.h, self.id, rung, a, dt, drag), "ct_drift")
+
+    def drift_lightcone(self, rung, a, dt, tau0, tau1, tau_max, nside, drag=0.0):
+        """Drift with the lightcone capture (cuda_drift with do_lc); returns this call's count."""
+        p = LcParams(tau0, tau1, tau_max, nside)
+        n = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.ct_drift_lightcone(self.ctx.h, self.id, rung, a, dt, drag, ctypes.byref(p), ctypes.byref(n)), "ct_drift_lightcone")
+        return n.value
+
+    def lightcone(self, clear=True):
+        """The captured entries (LC_ENTRY rows); clear empties the device buffer."""
+        n = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.ct_lightcone_count(self.ctx.h, self.id, ctypes.byref(n)), "ct_lightcone_count")
+        out = np.zeros(n.value, LC_ENTRY)
+        self.ctx.check(self.ctx.lib.ct_lightcone_download(self.ctx.h, self.id, _p(out), n.value, ctypes.byref(n), int(clear)), "ct_lightcone_download")
+        return out
+
+    def lightcone_reserve(self, entries):
+        self.ctx.check(self.ctx.lib.ct_lightcone_reserve(self.ctx.h, self.id, entries), "ct_lightcone_reserve")
 
     def tree(self):
         cnt = ctypes.c_int64()

@@ -23,6 +23,7 @@ UNITS = {
     "ct_api.cu": [],
     "ct_noalloc.cu": [],
     "ct_driver.cu": [],
+    "ct_lightcone.cu": [],
 }
 
 

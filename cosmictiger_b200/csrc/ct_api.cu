@@ -837,6 +837,7 @@ ct_status ct_box_destroy(ct_ctx* ctx, int box_id) {
 		return fail(c, CT_ERR_ARG, "ct_box_destroy: no such box");
 	}
 	cudaStreamSynchronize(c->stream);
+	lightcone_release(c, b);
 	const int64_t n = b->cap;
 	for (int d = 0; d < 3; d++) {
 		dfree(c, b->x[d], sizeof(uint32_t) * n);

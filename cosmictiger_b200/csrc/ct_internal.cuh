@@ -116,7 +116,17 @@ struct Box {
 	// kick results
 	ct_counters counters;
 	bool have_force = false;
+	// lightcone capture (ct_drift_lightcone): entries [0, lc_count) of lc
+	ct_lc_entry* lc = nullptr;
+	int64_t lc_cap = 0;
+	int64_t lc_count = 0;
+	uint32_t* lc_retry = nullptr;  // two lists of lc_retry_cap particle indices
+	int64_t lc_retry_cap = 0;
+	unsigned long long* d_lc_ctr = nullptr;  // [0] reserved entries, [1] first unfitted slot, [2] deferred particles
 };
+
+// Frees a box's lightcone buffers (ct_lightcone.cu).
+void lightcone_release(Ctx* c, Box* b);
 
 struct KickBuffers;  // interaction lists and expansions of the kick (ct_kick.cu)
 

@@ -170,6 +170,44 @@ ct_status ct_tree_create(ct_ctx* ctx, int box_id, const ct_tree_params* params, 
 ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* result);
 ct_status ct_drift(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag);
 
+/* ---- drift with the lightcone capture of cuda_drift (src/drift.cu:35-198) */
+
+/* One crossing of the light cone (lc_entry, cosmictiger/lightcone.hpp:54-58): the crossing point
+ * relative to the observer at the origin, fixed<int,31> (2^-31 box units, in [-1, 1]); the
+ * particle's velocity (code units, after drag); its HEALPix nested pixel at nside. */
+typedef struct {
+	int32_t x, y, z;
+	float vx, vy, vz;
+	int32_t pix;
+} ct_lc_entry;
+
+/* Lightcone of the drift (cuda_drift's tau0, tau1, tau_max and options lc_map_size): crossings of
+ * the period boundaries k * tau_max between tau0 and tau1 are recorded in the 8 periodic images
+ * next to the observer, when tau_max - tau1 < 1 (src/drift.cu:38). */
+typedef struct {
+	float tau0;
+	float tau1;
+	float tau_max;
+	int nside; /* 1 .. 8192 */
+} ct_lc_params;
+
+/* ct_drift plus the lightcone capture.  The crossings are appended to the box's lightcone buffer
+ * (grown as needed; no crossing is dropped); *captured (optional) receives this call's count.
+ * Waits for the drift to finish (the reference's cuda_drift synchronises the same way).
+ * Replaces cuda_drift(rung, a, dt, tau0, tau1, tau_max, drag) with options do_lc (drift.cu:156). */
+ct_status ct_drift_lightcone(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag, const ct_lc_params* lc, int64_t* captured);
+
+/* Entries held in the box's lightcone buffer. */
+ct_status ct_lightcone_count(ct_ctx* ctx, int box_id, int64_t* count);
+
+/* Copies up to max_entries entries (host memory) and, with clear != 0, empties the buffer;
+ * *count receives the number held before the call.  The order of entries within one drift is
+ * unspecified (the reference's is per block of its kernel). */
+ct_status ct_lightcone_download(ct_ctx* ctx, int box_id, ct_lc_entry* out, int64_t max_entries, int64_t* count, int clear);
+
+/* Sets the buffer's capacity in entries (at least what it holds); the drift grows it as needed. */
+ct_status ct_lightcone_reserve(ct_ctx* ctx, int box_id, int64_t entries);
+
 /* ---- hierarchical (multistep) step: kick_step_hierarchical (src/driver.cpp:382-593) */
 typedef struct {
 	int minrung;      /* the step's minimum rung */

@@ -1164,6 +1164,155 @@ void ct_or_drift(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, cons
 	}
 }
 
+// Bits 0..12 of v to the even bit positions 0..24.
+static uint32_t spread13(uint32_t v) {
+	uint32_t r = 0;
+	for (int b = 0; b < 13; b++) {
+		r |= ((v >> b) & 1u) << (2 * b);
+	}
+	return r;
+}
+
+// The HEALPix construction (Gorski et al. 2005, ApJ 622:759), as the reference evaluates it
+// (src/healpix.cu:55-171): face and in-face coordinates at the finest resolution 8192, the
+// nested index by bit interleaving (x on even bits), degraded to nside by integer division.
+int ct_or_healpix_nest(int nside, double x, double y, double z) {
+	const int NS = 8192;
+	const double piover2 = 0.5 * M_PI, twopi = 2.0 * M_PI;
+	const double zn = z / std::sqrt(x * x + y * y + z * z);
+	double phi = 0.0;
+	if (x != 0.0 || y != 0.0) {
+		phi = std::atan2(y, x);
+		if (phi < 0.0) {
+			phi += twopi;
+		}
+	}
+	const double za = std::fabs(zn);
+	const double tt = phi / piover2;
+	int face, ix, iy;
+	if (za <= 2. / 3.) {
+		const int jp = (int) std::floor(NS * (0.5 + tt - zn * 0.75));
+		const int jm = (int) std::floor(NS * (0.5 + tt + zn * 0.75));
+		const int ifp = jp / NS, ifm = jm / NS;
+		if (ifp == ifm) {
+			face = ifp % 4 + 4;
+		} else if (ifp < ifm) {
+			face = ifp % 4;
+		} else {
+			face = ifm % 4 + 8;
+		}
+		ix = jm % NS;
+		iy = NS - jp % NS - 1;
+	} else {
+		int ntt = (int) std::floor(tt);
+		if (ntt >= 4) {
+			ntt = 3;
+		}
+		const double tp = tt - ntt;
+		const double tmp = std::sqrt(3. * (1. - za));
+		const int jp = std::min((int) std::floor(NS * tp * tmp), NS - 1);
+		const int jm = std::min((int) std::floor(NS * (1. - tp) * tmp), NS - 1);
+		if (zn >= 0) {
+			face = ntt;
+			ix = NS - jm - 1;
+			iy = NS - jp - 1;
+		} else {
+			face = ntt + 8;
+			ix = jp;
+			iy = jm;
+		}
+	}
+	const int ipf = (int) (spread13(ix) | (spread13(iy) << 1));
+	const int f = NS / nside;
+	return ipf / (f * f) + face * nside * nside;
+}
+
+// fixed<int,31> = double (fixed.hpp:97-101): truncation of 2^31 x, saturating as the GPU's
+// conversion does at x = 1.
+static int32_t fixed31_from_double(double x) {
+	const double s = 2147483648.0 * x;
+	if (s >= 2147483647.0) {
+		return 2147483647;
+	}
+	return (int32_t) s;
+}
+
+int64_t ct_or_drift_lc(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt,
+		double drag, float tau0, float tau1, float tau_max, int nside, ct_or_lc_entry* out, int64_t max_out) {
+	// kernel arguments as cuda_drift passes them (src/drift.cu:156-197): floats widened to double
+	const double da = a, ddt = dt, t0 = tau0, t1 = tau1, tmax = tau_max;
+	const bool do_lc = tmax - t1 < 1.0;
+	const double c0 = 1.0 / tmax;
+	const double ainv = 1.0 / da;
+	const double c1 = ddt / da;
+	uint32_t* X[3] = { x, y, z };
+	int64_t count = 0;
+	for (int i = 0; i < n; i++) {
+		if (rung[i] != which_rung) {
+			continue;
+		}
+		float* vel = vxyz + 3 * i;
+		double p0[3], p1[3];
+		for (int d = 0; d < 3; d++) {
+			p0[d] = fixed32_to_double(X[d][i]);
+			p1[d] = p0[d] + double(vel[d]) * c1;
+		}
+		if (drag != 0.0) {
+			const double dc = 1.0 / (1.0 + drag * ddt);
+			for (int d = 0; d < 3; d++) {
+				vel[d] *= dc;
+			}
+		}
+		if (do_lc) {
+			for (int xi = -1; xi <= 0; xi++) {
+				for (int yi = -1; yi <= 0; yi++) {
+					for (int zi = -1; zi <= 0; zi++) {
+						const double A0[3] = { p0[0] + xi, p0[1] + yi, p0[2] + zi };
+						const double A1[3] = { p1[0] + xi, p1[1] + yi, p1[2] + zi };
+						const double dist0 = std::sqrt(A0[0] * A0[0] + A0[1] * A0[1] + A0[2] * A0[2]);
+						const double dist1 = std::sqrt(A1[0] * A1[0] + A1[1] * A1[1] + A1[2] * A1[2]);
+						const int i0 = (int) ((t0 + dist0) * c0);
+						const int i1 = (int) ((t1 + dist1) * c0);
+						if (i0 == i1 || !(dist1 <= 1.0 || dist0 <= 1.0)) {
+							continue;
+						}
+						// where the particle's straight path meets the light cone of period
+						// boundary (i0 + 1) tau_max: |X0 + v t| = ti - (tau0 + t), solved for t
+						const float vx = float(vel[0] * ainv), vy = float(vel[1] * ainv), vz = float(vel[2] * ainv);
+						const double ti = double(i0 + 1) * tmax;
+						const double sq = (ti - t0) * (ti - t0);
+						const double A = 1.0 - (vx * vx + vy * vy + vz * vz);
+						const double B = 2.0 * ((t0 - ti) - (vx * A0[0] + vy * A0[1] + vz * A0[2]));
+						const double C = sq - (A0[0] * A0[0] + A0[1] * A0[1] + A0[2] * A0[2]);
+						const double t = -(B + std::sqrt(B * B - 4.0 * A * C)) / (2.0 * A);
+						const double q[3] = { A0[0] + vx * t, A0[1] + vy * t, A0[2] + vz * t };
+						if (q[0] * q[0] + q[1] * q[1] + q[2] * q[2] <= 1.0) {
+							if (count < max_out) {
+								ct_or_lc_entry& e = out[count];
+								e.x = fixed31_from_double(q[0]);
+								e.y = fixed31_from_double(q[1]);
+								e.z = fixed31_from_double(q[2]);
+								e.vx = vel[0];
+								e.vy = vel[1];
+								e.vz = vel[2];
+								e.pix = ct_or_healpix_nest(nside, q[0], q[1], q[2]);
+							}
+							count++;
+						}
+					}
+				}
+			}
+		}
+		for (int d = 0; d < 3; d++) {
+			double v = p1[d];
+			v -= double(v >= 1.0);
+			v += double(v < 0.0);
+			X[d][i] = fixed32_from_double(v);
+		}
+	}
+	return count;
+}
+
 int ct_or_sort_by_rung(int n, int begin, int minrung, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung) {
 	if (minrung == 0) {
 		return 0;

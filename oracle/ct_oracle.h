@@ -88,6 +88,23 @@ int ct_or_kick_sampled(int order, const ct_or_kick_params* p, int nnodes, const 
 /* Drift of one rung (src/drift.cu:36-154, lightcone excluded). */
 void ct_or_drift(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt, double drag);
 
+/* Lightcone record of one crossing (lc_entry, cosmictiger/lightcone.hpp:54-58). */
+typedef struct {
+	int32_t x, y, z; /* fixed<int,31>: position of the crossing relative to the observer */
+	float vx, vy, vz;
+	int32_t pix; /* HEALPix nested pixel */
+} ct_or_lc_entry;
+
+/* HEALPix nested pixel of the direction (x, y, z) at nside (vec2pix_nest, src/healpix.cu:55-171). */
+int ct_or_healpix_nest(int nside, double x, double y, double z);
+
+/* Drift of one rung with the lightcone capture of cuda_drift_kernel (src/drift.cu:36-154):
+ * the particles' crossings of the light cone between tau0 and tau1 (period tau_max) in the 8
+ * periodic images next to the observer.  Writes at most max_out entries (in particle order,
+ * images in the reference's order) and returns how many crossings there were. */
+int64_t ct_or_drift_lc(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt,
+		double drag, float tau0, float tau1, float tau_max, int nside, ct_or_lc_entry* out, int64_t max_out);
+
 /* Rung partition of [begin, n): particles with rung >= minrung end up at [return, n)
  * (src/particles.cpp:1029-1076). */
 int ct_or_sort_by_rung(int n, int begin, int minrung, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung);

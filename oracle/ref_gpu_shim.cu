@@ -21,6 +21,7 @@
 #include <cosmictiger/cuda_mem.hpp>
 #include <cosmictiger/drift.hpp>
 #include <cosmictiger/ewald_indices.hpp>
+#include <cosmictiger/healpix.hpp>
 #include <cosmictiger/hpx.hpp>
 #include <cosmictiger/kick.hpp>
 #include <cosmictiger/lightcone.hpp>
@@ -32,6 +33,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "ct_gravity.h"
 
@@ -93,8 +95,21 @@ void cosmictiger_assert(const char* cond, bool ok, const char* file, int line) {
 	}
 }
 
-size_t lc_add_parts(const device_vector<device_vector<lc_entry>>&, double, double) {
-	return 0;  // lightcone capture is off (options.do_lc = false)
+// Where cuda_drift hands its per-block lightcone lists over (src/drift.cu:193): the harness
+// collects the entries (the lists live in the reference's managed heap, readable here after
+// the drift's synchronisation) instead of binning them into HEALPix maps and files.
+static std::vector<lc_entry> g_lc;
+
+size_t lc_add_parts(const device_vector<device_vector<lc_entry>>& entries, double, double) {
+	size_t count = 0;
+	for (int b = 0; b < entries.size(); b++) {
+		const auto& list = entries[b];
+		for (int j = 0; j < list.size(); j++) {
+			g_lc.push_back(list[j]);
+			count++;
+		}
+	}
+	return count;
 }
 
 // ---------------------------------------------------------------- harness
@@ -337,6 +352,53 @@ int ctref_drift(int64_t n, int64_t rung_begin, uint32_t* x, uint32_t* y, uint32_
 	if (e == cudaSuccess) {
 		get_particles(n, x, y, z, nullptr, nullptr);
 	}
+	free_particles();
+	g_rung_begin = 0;
+	return e == cudaSuccess ? 0 : -3;
+}
+
+// The reference's drift with its lightcone capture on (options do_lc, lc_map_size = nside;
+// create_glass selects its drag of pi, src/drift.cu:182): particles as in ctref_drift, the
+// velocities written back (the drag changes them), and the recorded entries copied to out
+// (at most max_out; *nout receives how many there were).  healpix_init fills the pixel tables
+// of vec2pix_nest as the reference's start-up does.
+int ctref_drift_lc(int64_t n, int64_t rung_begin, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int level, float a, float dt,
+		float tau0, float tau1, float tau_max, int nside, int create_glass, ct_lc_entry* out, int64_t max_out, int64_t* nout) {
+	if (!g_ready || n <= 0 || nside < 1 || nside > 8192) {
+		return -1;
+	}
+	healpix_init();
+	if (set_particles(n, x, y, z, vxyz, rung, false)) {
+		free_particles();
+		return -2;
+	}
+	g_rung_begin = rung_begin;
+	g_opts.do_lc = true;
+	g_opts.lc_map_size = nside;
+	g_opts.create_glass = create_glass != 0;
+	g_lc.clear();
+	cuda_drift((char) level, a, dt, tau0, tau1, tau_max, 0.0);
+	cudaError_t e = cudaGetLastError();
+	if (e == cudaSuccess) {
+		e = cudaDeviceSynchronize();
+	}
+	if (e == cudaSuccess) {
+		get_particles(n, x, y, z, vxyz, nullptr);
+		const int64_t m = std::min<int64_t>(max_out, (int64_t) g_lc.size());
+		for (int64_t i = 0; i < m; i++) {
+			const lc_entry& s = g_lc[i];
+			out[i].x = s.x.raw();
+			out[i].y = s.y.raw();
+			out[i].z = s.z.raw();
+			out[i].vx = s.vx;
+			out[i].vy = s.vy;
+			out[i].vz = s.vz;
+			out[i].pix = s.pix;
+		}
+		*nout = (int64_t) g_lc.size();
+	}
+	g_opts.do_lc = false;
+	g_opts.create_glass = false;
 	free_particles();
 	g_rung_begin = 0;
 	return e == cudaSuccess ? 0 : -3;

@@ -32,6 +32,10 @@ NODE_DTYPE = np.dtype(
 )
 
 
+# one lightcone crossing (ct_or_lc_entry / ct_lc_entry, the reference's lc_entry)
+LC_ENTRY = np.dtype([("x", "<i4"), ("y", "<i4"), ("z", "<i4"), ("vx", "<f4"), ("vy", "<f4"), ("vz", "<f4"), ("pix", "<i4")])
+
+
 class KickParams(ctypes.Structure):
     _fields_ = [
         ("sign", ctypes.c_float),
@@ -146,6 +150,24 @@ class Oracle:
     def drift(self, x, y, z, v, rung, which_rung, a, dt, drag=0.0):
         self.lib.ct_or_drift(ctypes.c_int(len(x)), _p(x), _p(y), _p(z), _p(v), _p(rung), ctypes.c_int(which_rung), ctypes.c_float(a),
                              ctypes.c_float(dt), ctypes.c_double(drag))
+
+    def healpix_nest(self, nside, x, y, z):
+        f = self.lib.ct_or_healpix_nest
+        f.restype = ctypes.c_int
+        return f(ctypes.c_int(nside), ctypes.c_double(x), ctypes.c_double(y), ctypes.c_double(z))
+
+    def drift_lc(self, x, y, z, v, rung, which_rung, a, dt, tau0, tau1, tau_max, nside, drag=0.0, max_out=None):
+        """Drift with the lightcone capture (in place); returns the entries (LC_ENTRY rows)."""
+        f = self.lib.ct_or_drift_lc
+        f.restype = ctypes.c_int64
+        cap = max_out if max_out is not None else 8 * len(x)
+        out = np.zeros(max(cap, 1), LC_ENTRY)
+        cnt = f(ctypes.c_int(len(x)), _p(x), _p(y), _p(z), _p(v), _p(rung), ctypes.c_int(which_rung), ctypes.c_float(a), ctypes.c_float(dt),
+                ctypes.c_double(drag), ctypes.c_float(tau0), ctypes.c_float(tau1), ctypes.c_float(tau_max), ctypes.c_int(nside), _p(out),
+                ctypes.c_int64(cap))
+        if cnt > cap:
+            raise RuntimeError("oracle lightcone: %d entries, room for %d" % (cnt, cap))
+        return out[:cnt]
 
     def sort_by_rung(self, x, y, z, v, rung, minrung, begin=0):
         return self.lib.ct_or_sort_by_rung(ctypes.c_int(len(x)), ctypes.c_int(begin), ctypes.c_int(minrung), _p(x), _p(y), _p(z), _p(v), _p(rung))

@@ -55,6 +55,28 @@ class ReferenceGPU:
             raise RuntimeError("reference kick failed (%d)" % rc)
         return {"v": v, "rung": r, "gx": g[0], "gy": g[1], "gz": g[2], "pot": g[3], "max_rung": int(ret[0]), "pot_sum": ret[1], "kin": ret[2]}
 
+    def drift_lc(self, x, y, z, v, rung, level, a, dt, tau0, tau1, tau_max, nside, create_glass=False, rung_begin=0, max_out=None):
+        """The reference's drift with its lightcone capture; returns (x, y, z, v, entries)."""
+        from tests.oracle_lib import LC_ENTRY
+
+        x, y, z = (np.ascontiguousarray(q, np.uint32).copy() for q in (x, y, z))
+        v = np.ascontiguousarray(v, np.float32).copy()
+        rung = np.ascontiguousarray(rung, np.int8)
+        cap = max_out if max_out is not None else 8 * len(x)
+        out = np.zeros(max(cap, 1), LC_ENTRY)
+        nout = ctypes.c_int64(0)
+        f = self.lib.ctref_drift_lc
+        f.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                      ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                      ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        rc = f(len(x), rung_begin, _p(x), _p(y), _p(z), _p(v), _p(rung), level, a, dt, tau0, tau1, tau_max, nside, int(create_glass), _p(out), cap,
+               ctypes.byref(nout))
+        if rc != 0:
+            raise RuntimeError("reference lightcone drift failed (%d)" % rc)
+        if nout.value > cap:
+            raise RuntimeError("reference lightcone: %d entries, room for %d" % (nout.value, cap))
+        return x, y, z, v, out[:nout.value]
+
     def drift(self, x, y, z, v, rung, level, a, dt, rung_begin=0):
         """Drift (in place on copies) the particles in [rung_begin, n) of rung `level`."""
         x, y, z = (np.ascontiguousarray(q, np.uint32).copy() for q in (x, y, z))
