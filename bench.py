@@ -56,11 +56,11 @@ def parse():
     ap.add_argument("--ensemble-nmin", type=int, default=16)
     ap.add_argument("--ensemble-nmax", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=3)
-    ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving", "lightcone"],
+    ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving", "lightcone", "fourier"],
                     help="instead of the benchmark line: precision (theta x order x summation, force error vs FP64 Ewald and "
                          "particle-steps/s), ensemble (512 boxes of 16^3..128^3, batched vs box by box, 20 steps) or serving "
                          "(Poisson arrivals of 32^3..256^3 requests, rate sweep, p50/p99 latency vs sequential runs) or lightcone "
-                         "(drift with the lightcone capture vs plain drift)")
+                         "(drift with the lightcone capture vs plain drift) or fourier (IC generator and power spectrum on an n^3 grid)")
     ap.add_argument("--study-seed", type=int, default=11)
     return ap.parse_args()
 
@@ -740,6 +740,9 @@ def study_lightcone(args, torch):
             e1.record(lib_stream)
             ctx.synchronize()
             torch.cuda.synchronize()
+            # the entries are handed over after every drift (the reference flushes its lists
+            # to the lightcone store each drift); here they are only dropped, untimed
+            box.lightcone_clear()
             if i >= 3:
                 ms.append(e0.elapsed_time(e1))
         return float(np.median(ms))
@@ -755,7 +758,6 @@ def study_lightcone(args, torch):
             counts.append(box.drift_lightcone(0, 1.0, dt, tau0, tau0 + dt, tau_max, nside))
 
         ms = timed(lc)
-        box.lightcone(clear=True)
         ent = float(np.mean(counts[3:]))
         gbs = (37.0 * N + 28.0 * ent) / (ms / 1e3) / 1e9
         rows.append({"nside": nside, "ms_per_drift": ms, "entries_per_drift": ent, "particles_s": N / (ms / 1e3), "achieved_gbs": gbs,
@@ -775,6 +777,63 @@ def study_lightcone(args, torch):
             "cpu_baseline": {"value": m / cpu_s, "unit": "particles/s", "cores": 1, "kind": "port", "sample": "%d particles, %d entries" % (m, len(ent))}}
 
 
+def study_fourier(args, torch):
+    """The IC generator and the power spectrum on an n^3 grid (default 256^3, box 500 Mpc, a
+    synthetic power.init-style table cut off at half the grid's Nyquist wavenumber): device time
+    per call (CUDA events on the library's stream around ct_initialize / ct_power_spectrum,
+    median of 5 after 2 warm-ups), particles per second, and the numpy restatement on 64^3 as
+    the CPU baseline (double-precision transforms, one process)."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import ics
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fourier_oracle as F
+
+    N, box = args.n, 500.0
+    cosmo = dict(omega_m=0.3111, z0=49.0, hubble=0.6732, sigma8=0.8607, H0=1.0)
+    k, P = ics.power_law_table(kcut=0.5 * np.pi * N / box / cosmo["hubble"])
+    ctx = ct.Context(order=7)
+    lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
+    b = ctx.box(N ** 3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        ms = []
+        for i in range(7):
+            ctx.synchronize()
+            e0.record(lib_stream)
+            fn()
+            e1.record(lib_stream)
+            ctx.synchronize()
+            torch.cuda.synchronize()
+            if i >= 2:
+                ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    rows = {}
+    for tw in (False, True):
+        ms = timed(lambda: b.initialize(N, box, k, P, twolpt=tw, **cosmo))
+        rows["initialize_2lpt" if tw else "initialize_zeldovich"] = {"ms": ms, "particles_s": N ** 3 / (ms / 1e3)}
+    ms = timed(lambda: b.power_spectrum(N, box, 1))
+    rows["power_spectrum"] = {"ms": ms, "particles_s": N ** 3 / (ms / 1e3)}
+    b.close()
+    ctx.close()
+    for key, r in rows.items():
+        print(json.dumps({key: r}), flush=True)
+    m = 64
+    km, Pm = ics.power_law_table(kcut=0.5 * np.pi * m / box / cosmo["hubble"])
+    t = time.perf_counter()
+    x, y, z, _, _ = F.initialize(m, box, cosmo["omega_m"], cosmo["z0"], cosmo["hubble"], cosmo["sigma8"], cosmo["H0"], km, Pm, True)
+    t_ic = time.perf_counter() - t
+    t = time.perf_counter()
+    F.power_spectrum(x, y, z, m, 1, box)
+    t_ps = time.perf_counter() - t
+    return {"study": "fourier", "grid": N, "particles": N ** 3, "box_mpc": box, "rows": rows,
+            "cpu_baseline": {"initialize_2lpt_particles_s": m ** 3 / t_ic, "power_spectrum_particles_s": m ** 3 / t_ps, "unit": "particles/s",
+                             "cores": 1, "kind": "port", "sample": "numpy restatement on %d^3" % m}}
+
+
 def peaks_hbm():
     try:
         with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
@@ -787,7 +846,7 @@ def run_study(args):
     import torch
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    fn = {"precision": study_precision, "ensemble": study_ensemble, "serving": study_serving, "lightcone": study_lightcone}[args.study]
+    fn = {"precision": study_precision, "ensemble": study_ensemble, "serving": study_serving, "lightcone": study_lightcone, "fourier": study_fourier}[args.study]
     t = time.perf_counter()
     res = fn(args, torch)
     res["wall_s"] = time.perf_counter() - t

@@ -126,6 +126,17 @@ class LcParams(ctypes.Structure):
     _fields_ = [("tau0", ctypes.c_float), ("tau1", ctypes.c_float), ("tau_max", ctypes.c_float), ("nside", ctypes.c_int)]
 
 
+class ICParams(ctypes.Structure):
+    _fields_ = [("nfour", ctypes.c_int), ("box_size", ctypes.c_double), ("omega_m", ctypes.c_double), ("z0", ctypes.c_double),
+                ("hubble", ctypes.c_double), ("sigma8", ctypes.c_double), ("H0", ctypes.c_double), ("twolpt", ctypes.c_int),
+                ("table_k", ctypes.c_void_p), ("table_p", ctypes.c_void_p), ("ntable", ctypes.c_int)]
+
+
+class ICReturn(ctypes.Structure):
+    _fields_ = [("D1", ctypes.c_double), ("D2", ctypes.c_double), ("prefac1", ctypes.c_double), ("prefac2", ctypes.c_double),
+                ("norm", ctypes.c_double), ("dxmax", ctypes.c_float * 3), ("dxmax2", ctypes.c_float * 3)]
+
+
 _lib = None
 
 
@@ -180,6 +191,9 @@ def library():
     L.ct_lightcone_count.argtypes = [vp, i32, ctypes.POINTER(i64)]
     L.ct_lightcone_download.argtypes = [vp, i32, vp, i64, ctypes.POINTER(i64), i32]
     L.ct_lightcone_reserve.argtypes = [vp, i32, i64]
+    L.ct_initialize.argtypes = [vp, i32, ctypes.POINTER(ICParams), ctypes.POINTER(ICReturn)]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.ct_power_spectrum.argtypes = [vp, i32, i32, i32, ctypes.c_double, i32, vp, vp, vp, ctypes.POINTER(i32)]
     _lib = L
     return L
 
@@ -377,6 +391,32 @@ class Box:
         out = np.zeros(n.value, LC_ENTRY)
         self.ctx.check(self.ctx.lib.ct_lightcone_download(self.ctx.h, self.id, _p(out), n.value, ctypes.byref(n), int(clear)), "ct_lightcone_download")
         return out
+
+    def initialize(self, nfour, box_size, table_k, table_p, omega_m=0.3111, z0=49.0, hubble=0.6732, sigma8=0.8607, H0=1.0, twolpt=True):
+        """Lattice + Zel'dovich (+ 2LPT) initial conditions from a power.init table (k in h/Mpc,
+        P in (Mpc/h)^3); returns the factors and largest displacements (ICReturn as a dict)."""
+        k = np.ascontiguousarray(table_k, np.float32)
+        P = np.ascontiguousarray(table_p, np.float32)
+        prm = ICParams(nfour, box_size, omega_m, z0, hubble, sigma8, H0, int(twolpt), _p(k).value, _p(P).value, len(k))
+        r = ICReturn()
+        self.ctx.check(self.ctx.lib.ct_initialize(self.ctx.h, self.id, ctypes.byref(prm), ctypes.byref(r)), "ct_initialize")
+        return {"D1": r.D1, "D2": r.D2, "prefac1": r.prefac1, "prefac2": r.prefac2, "norm": r.norm, "dxmax": list(r.dxmax), "dxmax2": list(r.dxmax2)}
+
+    def power_spectrum(self, nfour, box_size, fold=1):
+        """(k [1/Mpc], P, Perr) of the box's particles on an nfour^3 grid (power_spectrum_compute)."""
+        nb = ctypes.c_int()
+        self.ctx.check(self.ctx.lib.ct_power_spectrum(self.ctx.h, self.id, nfour, fold, box_size, 0, None, None, None, ctypes.byref(nb)),
+                       "ct_power_spectrum")
+        k, P, e = (np.zeros(nb.value, np.float32) for _ in range(3))
+        self.ctx.check(self.ctx.lib.ct_power_spectrum(self.ctx.h, self.id, nfour, fold, box_size, nb.value, _p(k), _p(P), _p(e), ctypes.byref(nb)),
+                       "ct_power_spectrum")
+        return k, P, e
+
+    def lightcone_clear(self):
+        """Empties the device buffer without copying it out."""
+        n = ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.ct_lightcone_download(self.ctx.h, self.id, None, 0, ctypes.byref(n), 1), "ct_lightcone_download")
+        return n.value
 
     def lightcone_reserve(self, entries):
         self.ctx.check(self.ctx.lib.ct_lightcone_reserve(self.ctx.h, self.id, entries), "ct_lightcone_reserve")

@@ -24,6 +24,7 @@ UNITS = {
     "ct_noalloc.cu": [],
     "ct_driver.cu": [],
     "ct_lightcone.cu": [],
+    "ct_fourier.cu": [],
 }
 
 
@@ -74,7 +75,7 @@ def build(verbose=False, force=False, jobs=None):
     if failed:
         raise RuntimeError("nvcc failed for " + ", ".join(failed))
     if force or _stale(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcufft"]
         subprocess.check_call(cmd)
     return LIB
 

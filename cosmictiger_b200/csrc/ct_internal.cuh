@@ -120,6 +120,7 @@ struct Box {
 	ct_lc_entry* lc = nullptr;
 	int64_t lc_cap = 0;
 	int64_t lc_count = 0;
+	int64_t lc_last = 0;           // entries of the last capturing drift (sizes the next one's room)
 	uint32_t* lc_retry = nullptr;  // two lists of lc_retry_cap particle indices
 	int64_t lc_retry_cap = 0;
 	unsigned long long* d_lc_ctr = nullptr;  // [0] reserved entries, [1] first unfitted slot, [2] deferred particles

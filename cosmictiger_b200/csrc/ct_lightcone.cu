@@ -297,7 +297,7 @@ void lightcone_release(Ctx* c, Box* b) {
 	b->lc = nullptr;
 	b->lc_retry = nullptr;
 	b->d_lc_ctr = nullptr;
-	b->lc_cap = b->lc_count = b->lc_retry_cap = 0;
+	b->lc_cap = b->lc_count = b->lc_last = b->lc_retry_cap = 0;
 }
 
 }  // namespace ct
@@ -343,8 +343,11 @@ extern "C" ct_status ct_drift_lightcone(ct_ctx* ctx, int box_id, int rung, float
 		CT_TRY(dalloc(c, (void**) &b->lc_retry, sizeof(uint32_t) * 2 * np, "lightcone deferred list"));
 		b->lc_retry_cap = np;
 	}
-	if (b->lc_cap == 0) {
-		CT_TRY(lc_resize(c, b, std::max<int64_t>(1 << 16, np / 64), 0));
+	// room for twice the last drift's crossings (at least 1/64 of the particles) before the
+	// launch, doubling the buffer, so that a steady run rarely defers particles
+	const int64_t room = std::max<int64_t>(std::max<int64_t>(1 << 16, np / 64), 2 * b->lc_last);
+	if (b->lc_cap - b->lc_count < room) {
+		CT_TRY(lc_resize(c, b, std::max<int64_t>(b->lc_count + room, 2 * b->lc_cap), b->lc_count));
 	}
 	LcArgs la;
 	la.b = b->rung_begin;
@@ -392,7 +395,7 @@ extern "C" ct_status ct_drift_lightcone(ct_ctx* ctx, int box_id, int rung, float
 		// slots [0, first unfitted) hold entries; the deferred particles need the rest
 		const int64_t written = (int64_t) h[1];
 		const int64_t need = (int64_t) h[0];
-		CT_TRY(lc_resize(c, b, std::max<int64_t>(need, b->lc_cap + b->lc_cap / 2), written));
+		CT_TRY(lc_resize(c, b, std::max<int64_t>(need + need / 2, 2 * b->lc_cap), written));
 		uint32_t* in = b->lc_retry + b->lc_retry_cap;
 		CT_CUDA(c, cudaMemcpyAsync(in, b->lc_retry, sizeof(uint32_t) * h[2], cudaMemcpyDeviceToDevice, st));
 		la.list = in;
@@ -403,6 +406,7 @@ extern "C" ct_status ct_drift_lightcone(ct_ctx* ctx, int box_id, int rung, float
 	cudaEventRecord(c->ev[7], st);
 	c->drift_timed = true;
 	b->lc_count = (int64_t) h[0];
+	b->lc_last = b->lc_count - before;
 	b->tree_valid = false;
 	if (captured) {
 		*captured = b->lc_count - before;

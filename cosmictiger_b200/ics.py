@@ -123,3 +123,21 @@ def softening(n_total, hsoft_spacing):
 def eta_default(eta=0.25):
     """eta / sqrt(self_phi) (src/options.cpp:166)."""
     return eta / np.sqrt(693.0 / 256.0)
+
+
+def read_power_init(path):
+    """The rows of a power.init file (two columns: k in h/Mpc, P in (Mpc/h)^3; the format
+    read_power_spectrum reads, src/initialize.cpp:853-880), as float32 arrays."""
+    rows = np.loadtxt(path, dtype=np.float64, ndmin=2)
+    return rows[:, 0].astype(np.float32), rows[:, 1].astype(np.float32)
+
+
+def power_law_table(kmin=1e-4, kmax=100.0, n=1024, index=-1.5, k0=0.1, bend=2.0, kcut=None):
+    """A smooth synthetic power.init-style table (k in h/Mpc, log-uniform): P = k / (1 + (k/k0)^bend)^((1 - index)/bend),
+    rising as k at large scales and falling as k^index at small ones; kcut multiplies it by
+    exp(-(k/kcut)^2) (power far below the grid scale)."""
+    k = np.exp(np.linspace(np.log(kmin), np.log(kmax), n))
+    P = 2e4 * (k / k0) / (1.0 + (k / k0) ** bend) ** ((1.0 - index) / bend)
+    if kcut is not None:
+        P = P * np.exp(-(k / kcut) ** 2) + 1e-30
+    return k.astype(np.float32), P.astype(np.float32)

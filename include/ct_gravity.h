@@ -208,6 +208,44 @@ ct_status ct_lightcone_download(ct_ctx* ctx, int box_id, ct_lc_entry* out, int64
 /* Sets the buffer's capacity in entries (at least what it holds); the drift grows it as needed. */
 ct_status ct_lightcone_reserve(ct_ctx* ctx, int box_id, int64_t entries);
 
+/* ---- initial conditions: Zel'dovich / 2LPT displacements of a lattice
+ * (initialize, src/initialize.cpp:261-355; the field of twolpt_generate, :416-535) */
+typedef struct {
+	int nfour;              /* particles per dimension = FFT grid (parts_dim = Nfour) */
+	double box_size;        /* box size in Mpc (code_to_cm / mpc_to_cm) */
+	double omega_m;         /* matter density (omega_b + omega_c) */
+	double z0;              /* starting redshift */
+	double hubble;          /* h */
+	double sigma8;          /* normalisation of the table */
+	double H0;              /* Hubble constant in code time units (constants::H0 code_to_s h) */
+	int twolpt;             /* add the second-order displacements */
+	const float* table_k;   /* power.init rows (read_power_spectrum, initialize.cpp:853-880): */
+	const float* table_p;   /*   k in h / Mpc, log-uniform; P in (Mpc / h)^3 */
+	int ntable;
+} ct_ic_params;
+
+typedef struct {
+	double D1, D2;          /* first- and second-order growth factors at z0 */
+	double prefac1, prefac2; /* velocity factors */
+	double norm;            /* sigma8 normalisation applied to the table */
+	float dxmax[3];         /* largest first-order displacement per axis, mean spacings */
+	float dxmax2[3];        /* largest second-order displacement per axis */
+} ct_ic_return;
+
+/* Fills a single box of nfour^3 particles with the lattice displaced by the Zel'dovich (and
+ * 2LPT) field of the table, seeded per k-space row as the reference seeds it (GSL taus).
+ * Replaces initialize(z0) with options Nfour, parts_dim, twolpt, sigma8, use_power_file. */
+ct_status ct_initialize(ct_ctx* ctx, int box_id, const ct_ic_params* params, ct_ic_return* result);
+
+/* ---- matter power spectrum (power_spectrum_compute, src/power.cpp:33-45; fft3d_power_spectrum,
+ * src/fft.cpp:172-214): cloud-kernel density on an nfour^3 grid after folding the box `fold`
+ * times, transform, window deconvolution, mean |delta_k|^2 in log-spaced shells from 1 to
+ * nfour / 2 (grid units).  k[i]: shell centre in 1 / Mpc (times fold); P[i]: mean power; Perr[i]
+ * (optional): the reference's error estimate.  *nbins receives the number of shells
+ * (max(nfour / 8, 64)); with k and P null only the count is returned. */
+ct_status ct_power_spectrum(ct_ctx* ctx, int box_id, int nfour, int fold, double box_size, int max_bins, float* k, float* P, float* Perr,
+		int* nbins);
+
 /* ---- hierarchical (multistep) step: kick_step_hierarchical (src/driver.cpp:382-593) */
 typedef struct {
 	int minrung;      /* the step's minimum rung */
