@@ -363,18 +363,22 @@ __global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float b
 
 }  // namespace
 
-ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag) {
+ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag, bool events) {
 	const double c1 = (double) dt / (double) a;
 	const double c0 = drag != 0.0 ? 1.0 / (1.0 + drag * (double) dt) : 1.0;
 	const int64_t np = b->n - b->rung_begin;
-	cudaEventRecord(c->ev[6], c->stream);
+	if (events) {
+		cudaEventRecord(c->ev[6], c->stream);
+	}
 	if (np > 0) {
 		c->launches++;
 		k_drift<<<grid(c, np, 256), 256, 0, c->stream>>>(b->rung_begin, b->n, b->x[0], b->x[1], b->x[2], b->v[0], b->v[1], b->v[2], b->rung, rung, c1, c0,
 				drag != 0.0);
 	}
-	cudaEventRecord(c->ev[7], c->stream);
-	c->drift_timed = true;
+	if (events) {
+		cudaEventRecord(c->ev[7], c->stream);
+		c->drift_timed = true;
+	}
 	CT_CUDA(c, cudaGetLastError());
 	b->tree_valid = false;
 	return CT_OK;

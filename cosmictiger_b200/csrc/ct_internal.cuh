@@ -121,9 +121,9 @@ struct Box {
 	int64_t lc_cap = 0;
 	int64_t lc_count = 0;
 	int64_t lc_last = 0;           // entries of the last capturing drift (sizes the next one's room)
-	uint32_t* lc_retry = nullptr;  // two lists of lc_retry_cap particle indices
-	int64_t lc_retry_cap = 0;
-	unsigned long long* d_lc_ctr = nullptr;  // [0] reserved entries, [1] first unfitted slot, [2] deferred particles
+	uint64_t* lc_cand = nullptr;   // candidate (particle, image) pairs of one drift
+	int64_t lc_cand_cap = 0;
+	unsigned long long* d_lc_ctr = nullptr;  // [0] candidates, [1] entries
 };
 
 // Frees a box's lightcone buffers (ct_lightcone.cu).
@@ -184,7 +184,7 @@ void* scratch(Ctx* c, int slot, size_t bytes, ct_status* st);
 // Translation-unit entry points.
 ct_status tree_build(Ctx* c, Box* b, const ct_tree_params* p);
 ct_status kick_run(Ctx* c, Box* b, const ct_kick_params* p, ct_kick_return* out);
-ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag);
+ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag, bool events = true);
 ct_status sort_by_rung_run(Ctx* c, Box* b, int min_rung);
 ct_status ewald_init(Ctx* c);
 ct_status step_hierarchical(Ctx* c, Box* b, const ct_step_params* p, ct_step_return* out);

@@ -8,10 +8,13 @@
 // the default FMA contraction, as the reference's drift.cu is), so that the recorded entries
 // are the reference's, bit for bit.
 //
-// Entries go to the box's lightcone buffer.  A warp reserves the entries of its particles with
-// one atomic; a particle whose entries do not fit is neither moved nor recorded but deferred
-// (index list), and the host grows the buffer to the exact need and runs the deferred particles
-// again: nothing is dropped and the buffer is sized by the crossings, not by a worst case.
+// Two passes ahead of the plain drift, so that the FP64 work runs on full warps: about one
+// particle in twenty crosses per drift, which would put a crossing in nearly every warp of a
+// fused kernel.  Pass 1 writes the (particle, image) pairs that a float pre-test cannot rule
+// out; the host sizes the entry buffer for them (nothing has moved, so an overfull candidate
+// list is simply redone after it grows); pass 2 runs the exact test and the pixel one pair per
+// lane and writes the entries; then k_drift moves the particles.  No crossing is dropped and
+// no worst-case buffer is held.
 #include "ct_internal.cuh"
 
 #include <algorithm>
@@ -80,9 +83,8 @@ __device__ int healpix_nest(int nside, double x, double y, double z) {
 }
 
 struct LcArgs {
-	int64_t b;               // range start (no list)
-	int64_t total;           // particles to visit: n - b, or the list's length
-	const uint32_t* list;    // deferred particles to visit again (null: the range)
+	int64_t b;               // range start
+	int64_t total;           // particles in the range
 	uint32_t* x[3];
 	float* v[3];
 	const int8_t* rung;
@@ -90,13 +92,10 @@ struct LcArgs {
 	double c1;               // dt / a
 	double drag_c0;          // 1 / (1 + drag dt)
 	int do_drag;
-	int do_lc;
 	double ainv, t0, t1, c0, tmax;  // 1 / a, tau0, tau1, 1 / tau_max, tau_max
 	int nside;
 	ct_lc_entry* out;
-	unsigned long long cap;
-	unsigned long long* ctr;  // [0] reserved entries, [1] first slot that did not fit, [2] deferred
-	uint32_t* defer;
+	unsigned long long* ctr;  // [0] candidates, [1] entries
 };
 
 // Crossing of periodic image `img` (x, y, z offsets -1 or 0; x slowest, the reference's loop
@@ -156,46 +155,46 @@ __device__ __forceinline__ bool lc_candidate(const LcArgs& a, const double p0[3]
 	return lo < 0.0 || floor(lo) != floor(hi);
 }
 
-__global__ void __launch_bounds__(LC_TPB) k_drift_lc(LcArgs a) {
+// The drift's start and end points and the velocity after drag of particle i, as cuda_drift
+// computes them (src/drift.cu:58-75): end = start + v dt / a in FP64, drag applied to v after.
+__device__ __forceinline__ void lc_particle(const LcArgs& a, int64_t i, double p0[3], double p1[3], float vel[3]) {
+#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		p0[d] = fixed_to_double(a.x[d][i]);
+		vel[d] = a.v[d][i];
+		p1[d] = __dadd_rn(p0[d], __dmul_rn((double) vel[d], a.c1));
+	}
+	if (a.do_drag) {
+#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			vel[d] = (float) ((double) vel[d] * a.drag_c0);
+		}
+	}
+}
+
+// Pass 1: the (particle, image) pairs that pass the pre-test, as index * 8 + image.  A warp
+// reserves its pairs with one atomic; pairs past the buffer are counted, not written (the host
+// then grows the buffer and runs the pass again: nothing has moved yet).
+__global__ void __launch_bounds__(LC_TPB) k_lc_candidates(LcArgs a, uint64_t* __restrict__ cand, unsigned long long cap) {
 	const int lane = threadIdx.x & 31;
 	const int64_t stride = (int64_t) gridDim.x * blockDim.x;
-	// warp-uniform trip count: the entry reservation below is a warp collective
+	// warp-uniform trip count: the reservation is a warp collective
 	for (int64_t w0 = blockIdx.x * (int64_t) blockDim.x + (threadIdx.x - lane); w0 < a.total; w0 += stride) {
-		const int64_t t = w0 + lane;
-		int64_t i = -1;
-		if (t < a.total) {
-			i = a.list ? (int64_t) a.list[t] : a.b + t;
-		}
-		bool act = i >= 0 && a.rung[i] == a.which;
-		double p0[3], p1[3];
-		float vel[3];
+		const int64_t i = a.b + w0 + lane;
 		unsigned mask = 0;
-		if (act) {
-#pragma unroll
-			for (int d = 0; d < 3; d++) {
-				p0[d] = fixed_to_double(a.x[d][i]);
-				vel[d] = a.v[d][i];
-				p1[d] = __dadd_rn(p0[d], __dmul_rn((double) vel[d], a.c1));
-			}
-			if (a.do_drag) {
-#pragma unroll
-				for (int d = 0; d < 3; d++) {
-					vel[d] = (float) ((double) vel[d] * a.drag_c0);
-				}
-			}
-			if (a.do_lc) {
-				// drift length, rounded up (relative 1e-6) past its float rounding
-				const float sx = (float) (p1[0] - p0[0]), sy = (float) (p1[1] - p0[1]), sz = (float) (p1[2] - p0[2]);
-				const float s = sqrtf(sx * sx + sy * sy + sz * sz) * 1.000001f;
-				for (int img = 0; img < 8; img++) {
-					double q[3];
-					if (lc_candidate(a, p0, s, img) && lc_crossing(a, p0, p1, vel, img, q)) {
-						mask |= 1u << img;
-					}
+		if (w0 + lane < a.total && a.rung[i] == a.which) {
+			double p0[3], p1[3];
+			float vel[3];
+			lc_particle(a, i, p0, p1, vel);
+			// drift length, rounded up (relative 1e-6) past its float rounding
+			const float sx = (float) (p1[0] - p0[0]), sy = (float) (p1[1] - p0[1]), sz = (float) (p1[2] - p0[2]);
+			const float s = sqrtf(sx * sx + sy * sy + sz * sz) * 1.000001f;
+			for (int img = 0; img < 8; img++) {
+				if (lc_candidate(a, p0, s, img)) {
+					mask |= 1u << img;
 				}
 			}
 		}
-		// one reservation per warp: inclusive prefix of the lanes' entry counts
 		const int cnt = __popc(mask);
 		int incl = cnt;
 #pragma unroll
@@ -204,58 +203,68 @@ __global__ void __launch_bounds__(LC_TPB) k_drift_lc(LcArgs a) {
 			incl += lane >= o ? y : 0;
 		}
 		const int wtot = __shfl_sync(0xffffffffu, incl, 31);
+		if (wtot == 0) {
+			continue;
+		}
 		unsigned long long base = 0;
-		if (wtot > 0) {
-			if (lane == 0) {
-				base = atomicAdd(a.ctr, (unsigned long long) wtot);
-			}
-			base = __shfl_sync(0xffffffffu, base, 0);
+		if (lane == 0) {
+			base = atomicAdd(a.ctr, (unsigned long long) wtot);
 		}
-		const unsigned long long mine = base + (unsigned long long) (incl - cnt);
-		if (act && cnt > 0 && mine + cnt > a.cap) {
-			// does not fit: leave the particle where it is and run it again after the host
-			// has grown the buffer
-			atomicMin(a.ctr + 1, mine);
-			const unsigned long long k = atomicAdd(a.ctr + 2, 1ull);
-			a.defer[k] = (uint32_t) i;
-			act = false;
-		}
-		if (act) {
-			unsigned long long k = mine;
-			for (int img = 0; img < 8; img++) {
-				if (mask >> img & 1u) {
-					double q[3];
-					lc_crossing(a, p0, p1, vel, img, q);
-					ct_lc_entry e;
-					// fixed<int,31> = double (fixed.hpp:97-101): truncation of 2^31 q
-					e.x = __double2int_rz(2147483648.0 * q[0]);
-					e.y = __double2int_rz(2147483648.0 * q[1]);
-					e.z = __double2int_rz(2147483648.0 * q[2]);
-					e.vx = vel[0];
-					e.vy = vel[1];
-					e.vz = vel[2];
-					e.pix = healpix_nest(a.nside, q[0], q[1], q[2]);
-					a.out[k++] = e;
+		base = __shfl_sync(0xffffffffu, base, 0);
+		unsigned long long k = base + (unsigned long long) (incl - cnt);
+		for (int img = 0; img < 8; img++) {
+			if (mask >> img & 1u) {
+				if (k < cap) {
+					cand[k] = ((uint64_t) i << 3) | (uint64_t) img;
 				}
-			}
-#pragma unroll
-			for (int d = 0; d < 3; d++) {
-				double x1d = p1[d];
-				x1d = __dsub_rn(x1d, (double) (x1d >= 1.0));
-				x1d = __dadd_rn(x1d, (double) (x1d < 0.0));
-				a.x[d][i] = fixed_from_double(x1d);
-				if (a.do_drag) {
-					a.v[d][i] = vel[d];
-				}
+				k++;
 			}
 		}
 	}
 }
 
-__global__ void k_lc_counters(unsigned long long* ctr, unsigned long long reserved) {
-	ctr[0] = reserved;
-	ctr[1] = ULLONG_MAX;
-	ctr[2] = 0;
+// Pass 2: the exact test of every candidate, one per lane; a crossing writes its entry.  The
+// buffer holds at least the candidates' count past the entries already there.
+__global__ void __launch_bounds__(LC_TPB) k_lc_entries(LcArgs a, const uint64_t* __restrict__ cand, int64_t ncand) {
+	const int lane = threadIdx.x & 31;
+	const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+	for (int64_t w0 = blockIdx.x * (int64_t) blockDim.x + (threadIdx.x - lane); w0 < ncand; w0 += stride) {
+		bool hit = false;
+		double q[3];
+		float vel[3];
+		if (w0 + lane < ncand) {
+			const uint64_t r = cand[w0 + lane];
+			double p0[3], p1[3];
+			lc_particle(a, (int64_t) (r >> 3), p0, p1, vel);
+			hit = lc_crossing(a, p0, p1, vel, (int) (r & 7), q);
+		}
+		const unsigned m = __ballot_sync(0xffffffffu, hit);
+		if (m == 0) {
+			continue;
+		}
+		unsigned long long base = 0;
+		if (lane == 0) {
+			base = atomicAdd(a.ctr + 1, (unsigned long long) __popc(m));
+		}
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if (hit) {
+			ct_lc_entry e;
+			// fixed<int,31> = double (fixed.hpp:97-101): truncation of 2^31 q
+			e.x = __double2int_rz(2147483648.0 * q[0]);
+			e.y = __double2int_rz(2147483648.0 * q[1]);
+			e.z = __double2int_rz(2147483648.0 * q[2]);
+			e.vx = vel[0];
+			e.vy = vel[1];
+			e.vz = vel[2];
+			e.pix = healpix_nest(a.nside, q[0], q[1], q[2]);
+			a.out[base + __popc(m & ((1u << lane) - 1u))] = e;
+		}
+	}
+}
+
+__global__ void k_lc_counters(unsigned long long* ctr, unsigned long long entries) {
+	ctr[0] = 0;
+	ctr[1] = entries;
 }
 
 // Entry buffer of at least `cap` entries holding the first `keep` entries of the old one.
@@ -292,12 +301,12 @@ Box* lc_box(Ctx* c, int id) {
 
 void lightcone_release(Ctx* c, Box* b) {
 	dfree(c, b->lc, sizeof(ct_lc_entry) * b->lc_cap);
-	dfree(c, b->lc_retry, sizeof(uint32_t) * 2 * b->lc_retry_cap);
+	dfree(c, b->lc_cand, sizeof(uint64_t) * b->lc_cand_cap);
 	dfree(c, b->d_lc_ctr, 4 * sizeof(unsigned long long));
 	b->lc = nullptr;
-	b->lc_retry = nullptr;
+	b->lc_cand = nullptr;
 	b->d_lc_ctr = nullptr;
-	b->lc_cap = b->lc_count = b->lc_last = b->lc_retry_cap = 0;
+	b->lc_cap = b->lc_count = b->lc_last = b->lc_cand_cap = 0;
 }
 
 }  // namespace ct
@@ -336,23 +345,18 @@ extern "C" ct_status ct_drift_lightcone(ct_ctx* ctx, int box_id, int rung, float
 	if (!b->d_lc_ctr) {
 		CT_TRY(dalloc(c, (void**) &b->d_lc_ctr, 4 * sizeof(unsigned long long), "lightcone counters"));
 	}
-	if (b->lc_retry_cap < np) {
-		dfree(c, b->lc_retry, sizeof(uint32_t) * 2 * b->lc_retry_cap);
-		b->lc_retry = nullptr;
-		b->lc_retry_cap = 0;
-		CT_TRY(dalloc(c, (void**) &b->lc_retry, sizeof(uint32_t) * 2 * np, "lightcone deferred list"));
-		b->lc_retry_cap = np;
-	}
-	// room for twice the last drift's crossings (at least 1/64 of the particles) before the
-	// launch, doubling the buffer, so that a steady run rarely defers particles
+	// candidate room: twice the last drift's crossings, at least 1/64 of the particles
 	const int64_t room = std::max<int64_t>(std::max<int64_t>(1 << 16, np / 64), 2 * b->lc_last);
-	if (b->lc_cap - b->lc_count < room) {
-		CT_TRY(lc_resize(c, b, std::max<int64_t>(b->lc_count + room, 2 * b->lc_cap), b->lc_count));
+	if (b->lc_cand_cap < room) {
+		dfree(c, b->lc_cand, sizeof(uint64_t) * b->lc_cand_cap);
+		b->lc_cand = nullptr;
+		b->lc_cand_cap = 0;
+		CT_TRY(dalloc(c, (void**) &b->lc_cand, sizeof(uint64_t) * room, "lightcone candidates"));
+		b->lc_cand_cap = room;
 	}
 	LcArgs la;
 	la.b = b->rung_begin;
 	la.total = np;
-	la.list = nullptr;
 	for (int d = 0; d < 3; d++) {
 		la.x[d] = b->x[d];
 		la.v[d] = b->v[d];
@@ -362,7 +366,6 @@ extern "C" ct_status ct_drift_lightcone(ct_ctx* ctx, int box_id, int rung, float
 	la.c1 = ddt / da;
 	la.do_drag = drag != 0.0;
 	la.drag_c0 = la.do_drag ? 1.0 / (1.0 + drag * ddt) : 1.0;
-	la.do_lc = 1;
 	la.ainv = 1.0 / da;
 	la.t0 = t0;
 	la.t1 = t1;
@@ -373,39 +376,43 @@ extern "C" ct_status ct_drift_lightcone(ct_ctx* ctx, int box_id, int rung, float
 	const int64_t before = b->lc_count;
 	cudaStream_t st = c->stream;
 	cudaEventRecord(c->ev[6], st);
-	c->launches++;
-	k_lc_counters<<<1, 1, 0, st>>>(b->d_lc_ctr, (unsigned long long) before);
-	unsigned long long h[3] = { 0, 0, 0 };
+	unsigned long long h[2] = { 0, 0 };
 	for (int pass = 0;; pass++) {
-		la.out = b->lc;
-		la.cap = (unsigned long long) b->lc_cap;
-		la.defer = b->lc_retry;  // first half: particles deferred by this pass
-		c->launches++;
-		k_drift_lc<<<lc_grid(c, la.total), LC_TPB, 0, st>>>(la);
+		c->launches += 2;
+		k_lc_counters<<<1, 1, 0, st>>>(b->d_lc_ctr, (unsigned long long) before);
+		k_lc_candidates<<<lc_grid(c, np), LC_TPB, 0, st>>>(la, b->lc_cand, (unsigned long long) b->lc_cand_cap);
 		CT_CUDA(c, cudaGetLastError());
-		CT_CUDA(c, cudaMemcpyAsync(h, b->d_lc_ctr, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+		CT_CUDA(c, cudaMemcpyAsync(h, b->d_lc_ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
 		CT_CUDA(c, cudaStreamSynchronize(st));
-		if (h[2] == 0) {
+		if ((int64_t) h[0] <= b->lc_cand_cap) {
 			break;
 		}
-		if (pass >= 3) {
-			// a deferred particle's entries fit after one growth; more passes mean a fault
-			return fail(c, CT_ERR_CUDA, "ct_drift_lightcone: deferred particles remain after the buffer grew");
+		if (pass >= 1) {
+			// the count of a pass that fits is the count of the one before
+			return fail(c, CT_ERR_CUDA, "ct_drift_lightcone: candidate count changed between passes");
 		}
-		// slots [0, first unfitted) hold entries; the deferred particles need the rest
-		const int64_t written = (int64_t) h[1];
-		const int64_t need = (int64_t) h[0];
-		CT_TRY(lc_resize(c, b, std::max<int64_t>(need + need / 2, 2 * b->lc_cap), written));
-		uint32_t* in = b->lc_retry + b->lc_retry_cap;
-		CT_CUDA(c, cudaMemcpyAsync(in, b->lc_retry, sizeof(uint32_t) * h[2], cudaMemcpyDeviceToDevice, st));
-		la.list = in;
-		la.total = (int64_t) h[2];
-		c->launches++;
-		k_lc_counters<<<1, 1, 0, st>>>(b->d_lc_ctr, (unsigned long long) written);
+		const int64_t need = (int64_t) h[0] + (int64_t) h[0] / 4;
+		dfree(c, b->lc_cand, sizeof(uint64_t) * b->lc_cand_cap);
+		b->lc_cand = nullptr;
+		b->lc_cand_cap = 0;
+		CT_TRY(dalloc(c, (void**) &b->lc_cand, sizeof(uint64_t) * need, "lightcone candidates"));
+		b->lc_cand_cap = need;
 	}
+	const int64_t ncand = (int64_t) h[0];
+	if (b->lc_cap - b->lc_count < ncand) {
+		CT_TRY(lc_resize(c, b, std::max<int64_t>(b->lc_count + ncand, 2 * b->lc_cap), b->lc_count));
+	}
+	la.out = b->lc;
+	if (ncand > 0) {
+		c->launches++;
+		k_lc_entries<<<lc_grid(c, ncand), LC_TPB, 0, st>>>(la, b->lc_cand, ncand);
+	}
+	CT_TRY(drift_run(c, b, rung, a, dt, drag, false));
+	CT_CUDA(c, cudaMemcpyAsync(h, b->d_lc_ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
 	cudaEventRecord(c->ev[7], st);
+	CT_CUDA(c, cudaStreamSynchronize(st));
 	c->drift_timed = true;
-	b->lc_count = (int64_t) h[0];
+	b->lc_count = (int64_t) h[1];
 	b->lc_last = b->lc_count - before;
 	b->tree_valid = false;
 	if (captured) {

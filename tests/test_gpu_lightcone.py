@@ -97,8 +97,8 @@ def test_lightcone_matches_oracle(ctx, oracle):
 
 
 def test_lightcone_buffer_growth_drops_nothing(ctx):
-    """A buffer far too small: the deferred particles run again after it grows; entries and
-    positions equal a run with room to spare, and entries accumulate over drifts."""
+    """An entry buffer far too small grows to the candidates' need before any entry is written;
+    entries and positions equal a run with room to spare, and entries accumulate over drifts."""
     st = _state(vscale=10.0)
     args = (0, 1.0, 0.05, 0.4, 0.45, 1.3, 32)
     o1, e1 = _drift(ctx, st, *args, reserve=4)
@@ -136,3 +136,23 @@ def test_lightcone_drift_equals_plain_drift(ctx):
     assert len(ent2) == 0
     for f in ("x", "y", "z", "v"):
         assert np.array_equal(out2[f], plain[f]), f
+
+
+def test_lightcone_many_candidates_first_drift(ctx, oracle):
+    """128^3 particles: the first drift's candidates overflow the initial candidate room, the
+    pass is redone after the list grows, and the entries still agree with the oracle's."""
+    x, y, z, v, _ = ics.zeldovich_lattice(128, index=-2.0, rms_spacing=0.25, seed=8)
+    v = (v * 10.0).astype(np.float32)
+    r = np.zeros(len(x), np.int8)
+    st = (x, y, z, v, r)
+    out, ent = _drift(ctx, st, 0, 1.0, 0.01, 0.62, 0.63, 1.5, 128)
+    xs, ys, zs, vs = (q.copy() for q in (x, y, z, v))
+    oent = oracle.drift_lc(xs, ys, zs, vs, r, 0, 1.0, 0.01, 0.62, 0.63, 1.5, 128)
+    print("lightcone 128^3: %d entries" % len(ent))
+    assert len(ent) > 70000
+    assert len(ent) == len(oent)
+    a_, b_ = _sorted(ent), _sorted(oent)
+    for f in ("x", "y", "z"):
+        assert np.max(np.abs(a_[f].astype(np.int64) - b_[f].astype(np.int64))) <= 2, f
+    assert np.mean(a_["pix"] == b_["pix"]) > 0.999
+    assert np.array_equal(out["x"], xs) and np.array_equal(out["y"], ys) and np.array_equal(out["z"], zs)
