@@ -1,8 +1,8 @@
 // Drift with the lightcone capture of the reference's cuda_drift_kernel (src/drift.cu:35-154).
 //
-// One pass over the rung's particles moves them (the FP64 update, wrap and fixed32 store of
-// k_drift) and records each crossing of the light cone in the 8 periodic images next to the
-// observer: the point where the particle's straight path meets the cone of the next period
+// The rung's particles move as k_drift moves them (the FP64 update, wrap and fixed32 store),
+// and each crossing of the light cone in the 8 periodic images next to the observer is
+// recorded: the point where the particle's straight path meets the cone of the next period
 // boundary (i0 + 1) tau_max, its velocity and its HEALPix nested pixel.  The crossing tests
 // and the solve keep the reference's expression forms in FP64 (this unit is compiled with
 // the default FMA contraction, as the reference's drift.cu is), so that the recorded entries
