@@ -417,6 +417,16 @@ __device__ __forceinline__ void warp_reduce_arr(float* L) {
 }
 
 // Ewald M2L for every node: dL = sum over the Ewald CC list.
+// Work units of a warp in a resident grid: lane 0 takes the next `chunk` units from the
+// counter, so that warps that finish early take more (tile costs vary with the leaf's size and
+// lists) and no partly filled last wave of blocks is left.
+__device__ __forceinline__ int64_t warp_take(unsigned long long* next, int chunk) {
+	unsigned long long v = 0;
+	if ((threadIdx.x & 31) == 0) {
+		v = atomicAdd(next, (unsigned long long) chunk);
+	}
+	return (int64_t) __shfl_sync(0xffffffffu, v, 0);
+}
 template<class Ops>
 __global__ void __launch_bounds__(128, 3) k_m2l_ewald(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi, const int2* __restrict__ ecc,
 		const int* __restrict__ ecc_list, float* __restrict__ dL, int do_phi, double* counters) {
@@ -430,9 +440,9 @@ __global__ void __launch_bounds__(128, 3) k_m2l_ewald(int64_t nn, const NodeW* _
 	__syncthreads();
 	const EwaldView<typename Ops::Tab> view { s_real, ct.four, ct.four_exp, ct.D0 };
 	const int lane = threadIdx.x & 31;
+	double icnt_tot = 0;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
-	double icnt_tot = 0;
 	for (int64_t si = gw; si < nn; si += nw) {
 		const int2 lst = ecc[si];
 		if (lst.y == 0) {
@@ -547,9 +557,9 @@ __global__ void __launch_bounds__(128) k_p2l(int64_t nn, const NodeW* __restrict
 		const uint32_t* __restrict__ x0, const uint32_t* __restrict__ x1, const uint32_t* __restrict__ x2, float* __restrict__ dL, double* counters) {
 	constexpr int NE = Ops::NEXP;
 	const int lane = threadIdx.x & 31;
+	double ncp = 0;
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
-	double ncp = 0;
 	for (int64_t si = gw; si < nn; si += nw) {
 		const int2 cpl = cp[si];
 		if (cpl.y == 0 || !(nodes[si].flags & 1)) {
@@ -685,6 +695,7 @@ struct P2PArgs {
 	int compensated;
 	double* pairs;
 	double* near_pairs;
+	unsigned long long* next;  // work counter: warps take tiles in list order
 };
 
 // Approximate reciprocal square root (the MUFU unit), flushing denormals: pair separations
@@ -883,11 +894,10 @@ template<bool SMALL>
 __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 	__shared__ P2PStage stage[P2P_TPB / 32];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nw = (gridDim.x * blockDim.x) >> 5;
 	P2PStage* my = &stage[w];
 	double npairs = 0.0, nnear = 0.0;
-	for (int64_t it = gw; it < a.nitems; it += nw) {
+	// a resident grid; each warp takes the next tile when it is done with one
+	for (int64_t it = warp_take(a.next, 1); it < a.nitems; it = warp_take(a.next, 1)) {
 		const int2 item = a.items[it];
 		const NodeW self = a.nodes[item.x];
 		const float h = a.sub_h ? a.sub_h[box_of(a.sub_off, a.nsub, self.pbeg)] : a.h;
@@ -1051,6 +1061,7 @@ struct KickTileArgs {
 	ct_kick_params kp;
 	double* sums;
 	int* max_rung;
+	unsigned long long* next;  // work counter (resident grid, tiles taken in list order)
 };
 
 // M2P, L2P and the kick for one 32-sink tile per warp (gravity.cu:157-211, kick.cu:53-177).
@@ -1061,15 +1072,13 @@ __global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
 	__shared__ double s_red[4][9];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nw = (gridDim.x * blockDim.x) >> 5;
 	const auto& kp = a.kp;
 	double acc[9];
 	for (int q = 0; q < 9; q++) {
 		acc[q] = 0.0;
 	}
 	int maxr = 0;
-	for (int64_t it = gw; it < a.nitems; it += nw) {
+	for (int64_t it = warp_take(a.next, 1); it < a.nitems; it = warp_take(a.next, 1)) {
 		const int2 item = a.items[it];
 		const NodeW self = a.nodes[item.x];
 		const int bx = a.nsub > 1 ? box_of(a.sub_off, a.nsub, self.pbeg) : 0;
@@ -1270,6 +1279,18 @@ __global__ void k_collect_leaves(int64_t nn, const NodeW* nodes, int64_t* leaves
 // ---------------------------------------------------------------- host driver
 }  // namespace
 
+// Blocks of `tpb` threads of `kernel` resident on the whole GPU (its register and shared
+// memory use decide; at least one per SM).
+template<class K>
+int resident_blocks(const Ctx* c, K kernel, int tpb) {
+	int nb = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, tpb, 0) != cudaSuccess || nb < 1) {
+		cudaGetLastError();
+		nb = 1;
+	}
+	return nb * c->nsm;
+}
+
 struct KickBuffers {
 	int2* per_node = nullptr;  // 7 arrays of nnodes
 	size_t per_node_n = 0;
@@ -1403,6 +1424,8 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		}
 		// ---- interactions
 		CT_CUDA(c, cudaMemsetAsync(counters, 0, 16 * sizeof(double), st));
+		// node-indexed kernels: a static interleave over all nodes (most hold no list of the
+		// kind; a work counter costs more here than the last wave's tail)
 		const int gm = c->nsm * 8;
 		c->launches++;
 		k_m2l_ewald<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL, kp->do_phi, counters);
@@ -1474,6 +1497,9 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			CT_TRY(s2);
 			unsigned long long* tcount = (unsigned long long*) (c->d_flags + 44);
 			CT_CUDA(c, cudaMemsetAsync(tcount, 0, 2 * sizeof(unsigned long long), st));
+			unsigned long long* wnext = (unsigned long long*) (c->d_flags + 52);  // work counters of the two launches
+			CT_CUDA(c, cudaMemsetAsync(wnext, 0, 2 * sizeof(unsigned long long), st));
+
 			c->launches++;
 			k_split_tiles<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 255) / 256, c->nsm * 8)), 256, 0, st>>>(items, nitems, b->nodes, tiles2,
 					tiles2 + nitems + 1, tcount);
@@ -1484,14 +1510,18 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			if (nbig > 0) {
 				pa.items = tiles2;
 				pa.nitems = nbig;
+				pa.next = wnext;
 				c->launches++;
-				k_p2p<false><<<(int) std::max<int64_t>(1, std::min<int64_t>((nbig + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
+				k_p2p<false><<<(int) std::max<int64_t>(1, std::min<int64_t>((nbig + 7) / 8, (int64_t) resident_blocks(c, k_p2p<false>, P2P_TPB))), P2P_TPB, 0,
+						st>>>(pa);
 			}
 			if (nsmall > 0) {
 				pa.items = tiles2 + nitems + 1;
 				pa.nitems = nsmall;
+				pa.next = wnext + 1;
 				c->launches++;
-				k_p2p<true><<<(int) std::max<int64_t>(1, std::min<int64_t>((nsmall + 7) / 8, (int64_t) c->nsm * 8)), P2P_TPB, 0, st>>>(pa);
+				k_p2p<true><<<(int) std::max<int64_t>(1, std::min<int64_t>((nsmall + 7) / 8, (int64_t) resident_blocks(c, k_p2p<true>, P2P_TPB))), P2P_TPB, 0,
+						st>>>(pa);
 			}
 			cudaEventRecord(c->ev[5], st);
 			KickTileArgs ka;
@@ -1524,8 +1554,11 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			ka.kp = *kp;
 			ka.sums = counters + 4;
 			ka.max_rung = c->d_flags + 48;
+			ka.next = (unsigned long long*) (c->d_flags + 62);
+			CT_CUDA(c, cudaMemsetAsync(ka.next, 0, sizeof(unsigned long long), st));
 			c->launches++;
-			k_leaf_kick<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 3) / 4, (int64_t) c->nsm * 16)), 128, 0, st>>>(ka);
+			k_leaf_kick<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 3) / 4, (int64_t) resident_blocks(c, k_leaf_kick<Ops>, 128))), 128, 0,
+					st>>>(ka);
 			cudaEventRecord(c->ev[12], st);
 		}
 		CT_CUDA(c, cudaGetLastError());
