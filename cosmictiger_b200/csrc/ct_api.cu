@@ -30,10 +30,13 @@ ct_status dalloc(Ctx* c, void** p, size_t bytes, const char* what) {
 	if (c->budget && c->used + bytes > c->budget) {
 		return fail(c, CT_ERR_MEMORY, std::string("HBM budget exhausted allocating ") + what);
 	}
-	const cudaError_t e = cudaMalloc(p, bytes);
+	// stream-ordered, from the context's pool: no device-wide synchronisation, and memory freed
+	// earlier in the context is reused without going back to the driver
+	const cudaError_t e = cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream);
 	if (e != cudaSuccess) {
 		cudaGetLastError();
-		return fail(c, CT_ERR_MEMORY, std::string("cudaMalloc failed for ") + what + ": " + cudaGetErrorString(e));
+		*p = nullptr;
+		return fail(c, CT_ERR_MEMORY, std::string("device allocation failed for ") + what + ": " + cudaGetErrorString(e));
 	}
 	c->used += bytes;
 	return CT_OK;
@@ -41,7 +44,7 @@ ct_status dalloc(Ctx* c, void** p, size_t bytes, const char* what) {
 
 void dfree(Ctx* c, void* p, size_t bytes) {
 	if (p) {
-		cudaFree(p);
+		cudaFreeAsync(p, c->stream);
 		c->used -= std::min(c->used, bytes == 0 ? size_t(16) : bytes);
 	}
 }
@@ -503,6 +506,20 @@ ct_status ct_ctx_create(ct_ctx** out, int device, size_t hbm_budget_bytes, int o
 		delete c;
 		return CT_ERR_CUDA;
 	}
+	// the context's device memory pool, keeping freed memory for reuse until the context ends
+	cudaMemPoolProps props = {};
+	props.allocType = cudaMemAllocationTypePinned;
+	props.handleTypes = cudaMemHandleTypeNone;
+	props.location.type = cudaMemLocationTypeDevice;
+	props.location.id = device;
+	if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess) {
+		cudaGetLastError();
+		cudaStreamDestroy(c->stream);
+		delete c;
+		return CT_ERR_CUDA;
+	}
+	uint64_t keep = UINT64_MAX;
+	cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
 	for (int i = 0; i < 16; i++) {
 		cudaEventCreate(&c->ev[i]);
 	}
@@ -515,7 +532,7 @@ ct_status ct_ctx_create(ct_ctx** out, int device, size_t hbm_budget_bytes, int o
 		ct_ctx_destroy((ct_ctx*) c);
 		return CT_ERR_MEMORY;
 	}
-	cudaMemset(c->d_flags, 0, 64 * sizeof(int));
+	cudaMemsetAsync(c->d_flags, 0, 64 * sizeof(int), c->stream);
 	const ct_status s = ewald_init(c);
 	if (s != CT_OK) {
 		ct_ctx_destroy((ct_ctx*) c);
@@ -550,6 +567,12 @@ void ct_ctx_destroy(ct_ctx* ctx) {
 	}
 	for (int i = 0; i < 16; i++) {
 		cudaEventDestroy(c->ev[i]);
+	}
+	if (c->stream) {
+		cudaStreamSynchronize(c->stream);
+	}
+	if (c->pool) {
+		cudaMemPoolDestroy(c->pool);  // returns the pool's memory to the driver
 	}
 	if (c->stream) {
 		cudaStreamDestroy(c->stream);
@@ -600,7 +623,7 @@ static ct_status box_create_impl(Ctx* c, int nsub, const int64_t* counts, int* b
 	if (s == CT_OK) {
 		s = dalloc(c, (void**) &b->d_sub_maxrung, sizeof(int) * nsub, "box max rungs");
 	}
-	if (s == CT_OK && cudaMemcpy(b->d_sub_off, b->sub_off.data(), sizeof(int64_t) * (nsub + 1), cudaMemcpyHostToDevice) != cudaSuccess) {
+	if (s == CT_OK && cudaMemcpyAsync(b->d_sub_off, b->sub_off.data(), sizeof(int64_t) * (nsub + 1), cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
 		s = fail(c, CT_ERR_CUDA, "copy of box offsets");
 	}
 	for (int d = 0; d < 3 && s == CT_OK; d++) {
@@ -674,8 +697,8 @@ ct_status ct_ensemble_set_params(ct_ctx* ctx, int box_id, const float* h, const 
 		CT_TRY(dalloc(c, (void**) &b->d_sub_GM, sizeof(float) * b->sub_cap, "box GM"));
 	}
 	b->sub_h_host.assign(h, h + b->nsub);
-	CT_CUDA(c, cudaMemcpy(b->d_sub_h, h, sizeof(float) * b->nsub, cudaMemcpyHostToDevice));
-	CT_CUDA(c, cudaMemcpy(b->d_sub_GM, GM, sizeof(float) * b->nsub, cudaMemcpyHostToDevice));
+	CT_CUDA(c, cudaMemcpyAsync(b->d_sub_h, h, sizeof(float) * b->nsub, cudaMemcpyHostToDevice, c->stream));
+	CT_CUDA(c, cudaMemcpyAsync(b->d_sub_GM, GM, sizeof(float) * b->nsub, cudaMemcpyHostToDevice, c->stream));
 	return CT_OK;
 }
 
@@ -784,7 +807,7 @@ ct_status ct_ensemble_reshape(ct_ctx* ctx, int box_id, int nbox, const int64_t* 
 	for (int s = 0; s < nbox; s++) {
 		b->sub_off[s + 1] = b->sub_off[s] + counts[s];
 	}
-	CT_CUDA(c, cudaMemcpy(b->d_sub_off, b->sub_off.data(), sizeof(int64_t) * (nbox + 1), cudaMemcpyHostToDevice));
+	CT_CUDA(c, cudaMemcpyAsync(b->d_sub_off, b->sub_off.data(), sizeof(int64_t) * (nbox + 1), cudaMemcpyHostToDevice, c->stream));
 	// the per-box softening, GM and first-call flags of the old layout no longer apply
 	if (b->d_sub_h) {
 		b->sub_h_host.clear();
@@ -813,7 +836,7 @@ ct_status ct_ensemble_set_first_call(ct_ctx* ctx, int box_id, const int* first_c
 	if (!b->d_sub_first) {
 		CT_TRY(dalloc(c, (void**) &b->d_sub_first, sizeof(int) * b->sub_cap, "box first-call flags"));
 	}
-	CT_CUDA(c, cudaMemcpy(b->d_sub_first, first_call, sizeof(int) * b->nsub, cudaMemcpyHostToDevice));
+	CT_CUDA(c, cudaMemcpyAsync(b->d_sub_first, first_call, sizeof(int) * b->nsub, cudaMemcpyHostToDevice, c->stream));
 	return CT_OK;
 }
 

@@ -137,6 +137,7 @@ struct Ctx {
 	int order = 7;
 	int nsm = 148;
 	cudaStream_t stream = nullptr;
+	cudaMemPool_t pool = nullptr;   // device memory of the context (stream-ordered on `stream`)
 	size_t budget = 0;
 	size_t used = 0;
 	std::string err;

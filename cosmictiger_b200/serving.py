@@ -54,8 +54,13 @@ def request_state(req):
 
 
 class Server:
-    def __init__(self, ctx, theta=0.55, hbm_budget=150e9, t0=1.0 / 64, bucket=128):
+    """Continuous batching.  Requests of at most `plain_above` particles advance together as one
+    ensemble per tick; larger ones advance as their own boxes in the same tick (batching gains
+    little for them and would cost a re-batch whenever membership changes)."""
+
+    def __init__(self, ctx, theta=0.55, hbm_budget=150e9, t0=1.0 / 64, bucket=128, plain_above=1 << 20):
         self.ctx = ctx
+        self.plain_above = plain_above
         self.theta = theta
         self.budget = hbm_budget
         self.t0 = t0
@@ -89,10 +94,13 @@ class Server:
                 keep.append(req)
         self.waiting = keep
 
-    def _ensemble(self):
-        members = [r.rid for r, _, _ in self.active]
+    def _batched(self, item):
+        return item[0].particles <= self.plain_above
+
+    def _ensemble(self, batched):
+        members = [r.rid for r, _, _ in batched]
         if members != self.ens_members:
-            counts = [r.particles for r, _, _ in self.active]
+            counts = [r.particles for r, _, _ in batched]
             if self.ens is None:
                 self.ens = self.ctx.ensemble(counts)
             else:
@@ -104,7 +112,7 @@ class Server:
             h = np.array([ics.softening(c, 0.02) for c in counts], np.float32)
             gm = np.array([1.0 / c for c in counts], np.float32)
             self.ens.set_box_params(h, gm)
-            self.ens_boxes = [b for _, b, _ in self.active]
+            self.ens_boxes = [b for _, b, _ in batched]
             self.ens.gather(self.ens_boxes)
             self.ens_dirty = False
             self.ens_members = members
@@ -112,14 +120,24 @@ class Server:
         return self.ens
 
     def tick(self, now_fn):
-        """One batched step of every active request; retire the finished ones."""
-        ens = self._ensemble()
-        # a request's first step is its run's first call (no ascending half kick)
-        ens.set_first_call([int(rem == r.steps) for r, _, rem in self.active])
-        ens.tree_create(self.theta, self.hmax, self.bucket)
-        ens.kick(KickParams.make(theta=self.theta, h=self.hmax, GM=1.0, eta=ics.eta_default(), t0=self.t0, first_call=False, save_force=False))
-        ens.drift(0, 1.0, self.t0)
-        self.ens_dirty = True
+        """One step of every active request; retire the finished ones."""
+        batched = [it for it in self.active if self._batched(it)]
+        if batched:
+            ens = self._ensemble(batched)
+            # a request's first step is its run's first call (no ascending half kick)
+            ens.set_first_call([int(rem == r.steps) for r, _, rem in batched])
+            ens.tree_create(self.theta, self.hmax, self.bucket)
+            ens.kick(KickParams.make(theta=self.theta, h=self.hmax, GM=1.0, eta=ics.eta_default(), t0=self.t0, first_call=False, save_force=False))
+            ens.drift(0, 1.0, self.t0)
+            self.ens_dirty = True
+        for req, box, rem in self.active:
+            if req.particles > self.plain_above:
+                # the plain path, exactly as run_sequential steps a request
+                h = ics.softening(req.particles, 0.02)
+                box.tree_create(self.theta, h, self.bucket)
+                box.kick(KickParams.make(theta=self.theta, h=h, GM=1.0 / req.particles, eta=ics.eta_default(), t0=self.t0, first_call=rem == req.steps,
+                                         save_force=False))
+                box.drift(0, 1.0, self.t0)
         self.ticks += 1
         done = []
         for item in self.active:
@@ -128,9 +146,11 @@ class Server:
             if item[2] == 0:
                 done.append(item)
         if done:
-            # bring every box's state back, then retire the finished requests
-            ens.scatter(self.ens_boxes)
-            self.ens_dirty = False
+            # bring the batched boxes' state back, then retire the finished requests
+            if any(self._batched(it) for it in done):
+                self.ens.scatter(self.ens_boxes)
+                self.ens_dirty = False
+                self.ens_members = None  # membership changes
             self.ctx.synchronize()
             t = now_fn()
             for item in done:
@@ -140,7 +160,6 @@ class Server:
                 box.close()
                 self.active.remove(item)
                 self.finished.append(req)
-            self.ens_members = None  # membership changed
 
     def run(self, requests, states, clock=time.perf_counter):
         """Serve an open-loop arrival sequence in real time; returns the finished requests."""

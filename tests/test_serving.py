@@ -6,7 +6,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_serving_results_same_alone_and_in_mix():
+@pytest.mark.parametrize("plain_above", [1 << 20, 14 ** 3])
+def test_serving_results_same_alone_and_in_mix(plain_above):
+    """All requests batched, and requests above 14^3 particles stepped as their own boxes."""
     import cosmictiger_b200 as ct
     from cosmictiger_b200 import serving
 
@@ -15,7 +17,7 @@ def test_serving_results_same_alone_and_in_mix():
     states = {r.rid: serving.request_state(r) for r in reqs}
     # a budget that admits about two of these requests at a time
     budget = 2.2 * max(r.particles for r in reqs) * serving.BYTES_PER_PARTICLE
-    srv = serving.Server(ctx, theta=0.55, hbm_budget=budget)
+    srv = serving.Server(ctx, theta=0.55, hbm_budget=budget, plain_above=plain_above)
     done = srv.run(reqs, states)
     assert len(done) == len(reqs)
     assert srv.ticks < sum(r.steps for r in reqs)  # some ticks advanced several requests

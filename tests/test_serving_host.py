@@ -5,10 +5,21 @@ from cosmictiger_b200 import serving
 
 
 class FakeBox:
-    def __init__(self, n):
+    def __init__(self, n, log=None):
         self.n = n
         self.steps = 0
         self.closed = False
+        self.log = log
+
+    # a box stepped on its own (the server's plain path)
+    def tree_create(self, *args):
+        pass
+
+    def kick(self, params):
+        self.log.append((self.steps == 0) == bool(params.first_call))
+
+    def drift(self, *args):
+        self.steps += 1
 
     def upload(self, *state):
         self.steps = 0
@@ -67,7 +78,7 @@ class FakeContext:
         self.peak = 0
 
     def box(self, n):
-        return FakeBox(n)
+        return FakeBox(n, self.log)
 
     def note(self, counts):
         self.peak = max(self.peak, sum(counts))
@@ -94,3 +105,21 @@ def test_server_steps_and_budget():
     assert all(ctx.log) and len(ctx.log) == sum(r.steps for r in reqs)
     assert ctx.peak * serving.BYTES_PER_PARTICLE <= budget
     assert srv.ticks < sum(r.steps for r in reqs)
+
+
+def test_server_plain_path_for_large_requests():
+    """Requests above plain_above step as their own boxes in the same ticks as the batched
+    ones: exact step counts and first-call flags for both kinds; the ensemble holds only the
+    small ones."""
+    reqs = serving.poisson_requests(40, rate=5000.0, nmin=8, nmax=20, smin=1, smax=9, seed=12)
+    states = {r.rid: () for r in reqs}
+    cut = 12 ** 3
+    assert any(r.particles > cut for r in reqs) and any(r.particles <= cut for r in reqs)
+    ctx = FakeContext()
+    srv = serving.Server(ctx, hbm_budget=1e18, plain_above=cut)
+    done = srv.run(reqs, states)
+    assert sorted(r.rid for r in done) == list(range(len(reqs)))
+    for r in done:
+        assert r.result["steps"] == r.steps, (r.rid, r.result, r.steps)
+    assert all(ctx.log) and len(ctx.log) == sum(r.steps for r in reqs)
+    assert ctx.peak <= sum(r.particles for r in reqs if r.particles <= cut)
