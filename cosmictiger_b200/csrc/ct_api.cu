@@ -31,7 +31,7 @@ ct_status dalloc(Ctx* c, void** p, size_t bytes, const char* what) {
 		return fail(c, CT_ERR_MEMORY, std::string("HBM budget exhausted allocating ") + what);
 	}
 	// stream-ordered, from the context's pool: no device-wide synchronisation, and memory freed
-	// earlier in the context is reused without going back to the driver
+	// earlier in the context is reused without going back to the CUDA driver
 	const cudaError_t e = cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream);
 	if (e != cudaSuccess) {
 		cudaGetLastError();
@@ -572,7 +572,7 @@ void ct_ctx_destroy(ct_ctx* ctx) {
 		cudaStreamSynchronize(c->stream);
 	}
 	if (c->pool) {
-		cudaMemPoolDestroy(c->pool);  // returns the pool's memory to the driver
+		cudaMemPoolDestroy(c->pool);  // returns the pool's memory to the CUDA driver
 	}
 	if (c->stream) {
 		cudaStreamDestroy(c->stream);

@@ -10,8 +10,8 @@ the next tick.  Results do not depend on the mix: boxes of an ensemble never int
 every kernel treats them independently, so a request's result is bit-identical alone and
 batched with others.
 
-The reference has no serving layer; this follows the north-star description of request
-admission by HBM budget, device-resident state and p50/p99 latency reporting.
+The reference has no serving layer; this one admits requests by a device-memory budget,
+keeps their state resident on the device between steps and reports p50/p99 latency.
 """
 import time
 from dataclasses import dataclass, field
