@@ -763,6 +763,9 @@ extern "C" ct_status ct_power_spectrum(ct_ctx* ctx, int box_id, int nfour, int f
 		return fail(c, CT_ERR_ARG, "ct_power_spectrum: bad arguments");
 	}
 	Box* b = c->boxes[box_id];
+	if (b->nsub != 1) {
+		return fail(c, CT_ERR_ARG, "ct_power_spectrum: the spectrum is of a single box, not an ensemble");
+	}
 	const int N = nfour;
 	if (N < 4 || N > 2048 || N % 2 != 0 || fold < 1 || !(box_size > 0.0)) {
 		return fail(c, CT_ERR_ARG, "ct_power_spectrum: nfour must be even, 4 .. 2048; fold >= 1; box_size > 0");
