@@ -610,8 +610,9 @@ extern "C" ct_status ct_initialize(ct_ctx* ctx, int box_id, const ct_ic_params* 
 	}
 	Box* b = c->boxes[box_id];
 	const int N = p->nfour;
-	if (N < 4 || N > 2048 || N % 2 != 0) {
-		return fail(c, CT_ERR_ARG, "ct_initialize: nfour must be even, 4 .. 2048");
+	if (N < 4 || N > 1024 || N % 2 != 0) {
+		// (cuFFT's 3-D plans take 32-bit sizes)
+		return fail(c, CT_ERR_ARG, "ct_initialize: nfour must be even, 4 .. 1024");
 	}
 	const int64_t n = (int64_t) N * N * N;
 	if (b->nsub != 1 || b->n != n) {
@@ -767,8 +768,8 @@ extern "C" ct_status ct_power_spectrum(ct_ctx* ctx, int box_id, int nfour, int f
 		return fail(c, CT_ERR_ARG, "ct_power_spectrum: the spectrum is of a single box, not an ensemble");
 	}
 	const int N = nfour;
-	if (N < 4 || N > 2048 || N % 2 != 0 || fold < 1 || !(box_size > 0.0)) {
-		return fail(c, CT_ERR_ARG, "ct_power_spectrum: nfour must be even, 4 .. 2048; fold >= 1; box_size > 0");
+	if (N < 4 || N > 1024 || N % 2 != 0 || fold < 1 || !(box_size > 0.0)) {
+		return fail(c, CT_ERR_ARG, "ct_power_spectrum: nfour must be even, 4 .. 1024; fold >= 1; box_size > 0");
 	}
 	// log-spaced bin edges in grid units from 1 to N / 2 (fft3d_power_spectrum, fft.cpp:172-214)
 	std::vector<float> kb;

@@ -15,6 +15,9 @@
  *                        src/kick.cu:179-609 (cuda_execute_kicks)
  *   drift                cosmictiger/drift.hpp:51-54, src/drift.cu:36-185
  *   ewald_const::init    cosmictiger/ewald_indices.hpp:32-41, src/ewald_indices.cu:30-114
+ *   drift with lightcone src/drift.cu:35-198 (do_lc), src/healpix.cu:55-171, lc_add_parts input
+ *   initialize           src/initialize.cpp:261-355 (Zel'dovich / 2LPT from power.init)
+ *   power spectrum       src/power.cpp:33-77, src/power.cu:32-85, src/fft.cpp:172-360
  */
 #ifndef CT_GRAVITY_H
 #define CT_GRAVITY_H
@@ -211,7 +214,7 @@ ct_status ct_lightcone_reserve(ct_ctx* ctx, int box_id, int64_t entries);
 /* ---- initial conditions: Zel'dovich / 2LPT displacements of a lattice
  * (initialize, src/initialize.cpp:261-355; the field of twolpt_generate, :416-535) */
 typedef struct {
-	int nfour;              /* particles per dimension = FFT grid (parts_dim = Nfour) */
+	int nfour;              /* particles per dimension = FFT grid (parts_dim = Nfour), even, 4 .. 1024 */
 	double box_size;        /* box size in Mpc (code_to_cm / mpc_to_cm) */
 	double omega_m;         /* matter density (omega_b + omega_c) */
 	double z0;              /* starting redshift */
@@ -238,7 +241,7 @@ typedef struct {
 ct_status ct_initialize(ct_ctx* ctx, int box_id, const ct_ic_params* params, ct_ic_return* result);
 
 /* ---- matter power spectrum (power_spectrum_compute, src/power.cpp:33-45; fft3d_power_spectrum,
- * src/fft.cpp:172-214): cloud-kernel density on an nfour^3 grid after folding the box `fold`
+ * src/fft.cpp:172-214): cloud-kernel density on an nfour^3 grid (nfour even, 4 .. 1024) after folding the box `fold`
  * times, transform, window deconvolution, mean |delta_k|^2 in log-spaced shells from 1 to
  * nfour / 2 (grid units).  k[i]: shell centre in 1 / Mpc (times fold); P[i]: mean power; Perr[i]
  * (optional): the reference's error estimate.  *nbins receives the number of shells
