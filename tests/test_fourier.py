@@ -83,3 +83,34 @@ def test_displacements_first_order_dominate_with_a_cut_spectrum():
     d1, d2 = disp(a[0]), disp(b[0])
     assert 0.005 < np.sqrt(np.mean(d1 ** 2)) < 0.5
     assert np.sqrt(np.mean((d2 - d1) ** 2)) < 0.05 * np.sqrt(np.mean(d1 ** 2))
+
+
+def test_sigma8_normalisation_by_independent_quadrature():
+    """The normalised table's top-hat variance at R = 8/h Mpc, integrated by adaptive quadrature
+    over the same k range, is sigma8^2 (the restated Simpson sum, initialize.cpp:140-173)."""
+    from scipy import integrate
+
+    k, P = ics.power_law_table()
+    h, s8 = 0.6732, 0.8607
+    Pn, lkmin, dlk, lkmax, _ = F.power_table(k, P, h, s8)
+    R = 8.0 / h
+
+    def f(lk):
+        kk = np.exp(lk)
+        x = kk * R
+        W = 3 * (np.sin(x) - x * np.cos(x)) / x ** 3
+        return kk ** 3 * F.interp_power(Pn, lkmin, dlk, np.array([kk]))[0] * W * W / (2 * np.pi ** 2)
+
+    val, _ = integrate.quad(f, lkmin + 1.5 * dlk, lkmax - 2.5 * dlk, limit=2000)
+    assert abs(np.sqrt(val) / s8 - 1) < 1e-6
+
+
+@pytest.mark.parametrize("kh", [0.3, 1.0, 2.0, 3.0])
+def test_cloud_kernel_window_is_sinc6(kh):
+    """The continuous Fourier transform of the quintic cloud kernel is sinc(k/2)^6, the window
+    whose inverse (cloud_filter) the IC generator and the power spectrum apply."""
+    from scipy import integrate
+
+    ft, _ = integrate.quad(lambda x: F.cloud_weight(np.array([x]))[0] * np.cos(kh * x), -3, 3, limit=200)
+    assert abs(ft - np.sinc(kh / 2 / np.pi) ** 6) < 1e-8
+    assert abs(F.cloud_filter(np.array([kh]))[0] * ft - 1) < 1e-7
