@@ -114,3 +114,20 @@ def test_cloud_kernel_window_is_sinc6(kh):
     ft, _ = integrate.quad(lambda x: F.cloud_weight(np.array([x]))[0] * np.cos(kh * x), -3, 3, limit=200)
     assert abs(ft - np.sinc(kh / 2 / np.pi) ** 6) < 1e-8
     assert abs(F.cloud_filter(np.array([kh]))[0] * ft - 1) < 1e-7
+
+
+@pytest.mark.parametrize("a", [0.02, 0.1, 0.3, 0.6])
+def test_growth_factor_fit_against_exact_growth(a):
+    """The growth factor's fitting formula (cosmos_growth_factor, cosmology.cpp:80-87), normalised
+    to a = 1, follows the exact flat-LCDM linear growth D(a) ~ H(a) int da / (a H)^3 within 0.3%."""
+    from scipy import integrate
+
+    om = 0.3111
+
+    def exact(x):
+        E = lambda u: np.sqrt(om / u ** 3 + 1 - om)  # noqa: E731
+        val, _ = integrate.quad(lambda u: 1.0 / (u * E(u)) ** 3, 0, x)
+        return 2.5 * om * E(x) * val
+
+    fit = F.growth_factor(om, a) / F.growth_factor(om, 1.0)
+    assert abs(fit / (exact(a) / exact(1.0)) - 1) < 3e-3
