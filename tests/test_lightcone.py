@@ -96,3 +96,39 @@ def test_lightcone_oracle_same_drift_as_plain(oracle):
     # no capture when tau_max - tau1 >= 1 (src/drift.cu:38)
     c = [q.copy() for q in (x, y, z, v)]
     assert len(oracle.drift_lc(*c, r, 2, 0.8, 0.04, 0.1, 0.14, 1.2, 8)) == 0
+
+
+def _pix2vec_nest(nside, p):
+    """Centre of nested pixel p (the inverse construction of Gorski et al. 2005): face and
+    in-face (ix, iy) from the bits, ring and longitude index from the face's base ring and
+    longitude, then z and phi of the ring position."""
+    jrll = [2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4]
+    jpll = [1, 3, 5, 7, 0, 2, 4, 6, 1, 3, 5, 7]
+    face, ipf = divmod(p, nside * nside)
+    ix = iy = 0
+    for b in range(16):
+        ix |= ((ipf >> (2 * b)) & 1) << b
+        iy |= ((ipf >> (2 * b + 1)) & 1) << b
+    jr = jrll[face] * nside - ix - iy - 1
+    if jr < nside:
+        nr, z, kshift = jr, 1 - jr * jr / (3.0 * nside * nside), 0
+    elif jr > 3 * nside:
+        nr = 4 * nside - jr
+        z, kshift = -1 + nr * nr / (3.0 * nside * nside), 0
+    else:
+        nr, z, kshift = nside, (2 * nside - jr) * 2.0 / (3.0 * nside), (jr - nside) & 1
+    jp = (jpll[face] * nr + ix - iy + 1 + kshift) // 2
+    if jp > 4 * nside:
+        jp -= 4 * nside
+    if jp < 1:
+        jp += 4 * nside
+    phi = (jp - (kshift + 1) * 0.5) * (np.pi / 2 / nr)
+    st = np.sqrt(max(0.0, 1 - z * z))
+    return st * np.cos(phi), st * np.sin(phi), z
+
+
+@pytest.mark.parametrize("nside", [1, 2, 4, 8, 16])
+def test_healpix_pixel_centres_round_trip(oracle, nside):
+    """Every pixel's centre, from the independent inverse construction, lies in that pixel."""
+    for p in range(12 * nside * nside):
+        assert oracle.healpix_nest(nside, *_pix2vec_nest(nside, p)) == p, (nside, p)
