@@ -442,7 +442,9 @@ def main():
     if args.ensemble_boxes > 0:
         ens_res = ensemble_compare(ct, torch, ctx, args, theta, lib_stream)
     acc = None
-    if args.accuracy_sinks and rank == 0:
+    if args.accuracy_sinks:
+        # every rank checks its own box (rank 0 reports), so that no rank waits at the barrier
+        # below for another's check
         acc = accuracy(box, args.accuracy_sinks, h, N)
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
