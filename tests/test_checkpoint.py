@@ -99,3 +99,23 @@ def test_resume_hierarchical_run_from_checkpoint(tmp_path):
     assert a.rung_state() == b.rung_state()
     assert sa == sb
     ctx.close()
+
+
+def test_layouts_match_the_reference_compiler():
+    """The record layouts used here equal the reference's as its compiler lays them out
+    (tests/golden/ref_layouts.json, printed by oracle/layout_probe.cu built against the
+    reference's headers): driver_params, domain_t and the lightcone's lc_entry."""
+    import json
+    import os
+
+    import cosmictiger_b200 as ct
+
+    ref = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_layouts.json")))
+    d, dp = ck.DRIVER_PARAMS, ref["driver_params"]
+    assert d.itemsize == dp["size"]
+    for f in ("energies", "max_rung", "bucket_size", "total_processed", "flops", "itime"):
+        assert d.fields[f][1] == dp[f], f
+    assert ck.DOMAIN_ENTRY.itemsize == 8 + ref["domain_t"]  # pair<size_t key, domain_t>
+    lc = ct.LC_ENTRY
+    assert lc.itemsize == ref["lc_entry"]["size"]
+    assert lc.fields["vx"][1] == ref["lc_entry"]["vx"] and lc.fields["pix"][1] == ref["lc_entry"]["pix"]
