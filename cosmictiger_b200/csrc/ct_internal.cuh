@@ -14,7 +14,7 @@ constexpr int MAX_ORDER_NEXP = 50;   // order-7 local expansion
 constexpr int MAX_ORDER_NMULT = 37;  // order-7 multipole
 constexpr int NMULT_STRIDE = 40;     // multipole stride in floats (16-byte aligned rows)
 constexpr int NEXP_STRIDE = 52;      // expansion stride in floats (16-byte aligned rows)
-constexpr int MAX_DEPTH = 128;       // cosmictiger/defs.hpp:77
+constexpr int MAX_DEPTH = 128;       // cosmictiger/defs.hpp:86
 constexpr int WARP = 32;
 constexpr int MIN_PARTS_PCCP = 38;   // src/kick.cu:32
 

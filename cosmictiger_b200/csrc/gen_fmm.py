@@ -18,12 +18,12 @@ Lengths are scaled by 1e3 inside every operator (the reference's SCALE_FACTOR,
 ``cosmictiger/fmm_kernels.hpp:33-49``) so that high powers stay in float range.
 
 Operators (mathematics restated from ``src/fmm_kernel_codegen.cpp``):
-  greens      D(n)  = d^n(-1/r)                                   (codegen.cpp:1320-1370)
-  ewald_*     periodic correction d^n(phi_ewald + 1/r)            (codegen.cpp:1040-1233)
-  m2l         L(n) += sum_m M(m) D(n+m) / m!                      (codegen.cpp:1374-1497)
-  p2m         M(n)  = detrace((-x)^n) / (2|n|-1)!!  (|n|>=3)      (codegen.cpp:1499-1515)
-  m2m         M'(n) = detrace(sum_k C(n,k) (-d)^(n-k) M(k))       (codegen.cpp:1517-1610)
-  l2l / l2p   L'(n) = sum_k d^k/k! L(n+k)                         (codegen.cpp:715-850)
+  greens      D(n)  = d^n(-1/r)                                   (codegen.cpp:1265-1306)
+  ewald_*     periodic correction d^n(phi_ewald + 1/r)            (codegen.cpp:1036-1216)
+  m2l         L(n) += sum_m M(m) D(n+m) / m!                      (codegen.cpp:1311-1451)
+  p2m         M(n)  = detrace((-x)^n) / (2|n|-1)!!  (|n|>=3)      (codegen.cpp:1455-1471)
+  m2m         M'(n) = detrace(sum_k C(n,k) (-d)^(n-k) M(k))       (codegen.cpp:1473-1586)
+  l2l / l2p   L'(n) = sum_k d^k/k! L(n+k)                         (codegen.cpp:683-834)
 The code emitted here is this project's own; only the mathematical definitions
 and the storage layout are shared with the reference.
 """

@@ -15,7 +15,7 @@
  *                        src/kick.cu:179-609 (cuda_execute_kicks)
  *   drift                cosmictiger/drift.hpp:51-54, src/drift.cu:36-185
  *   ewald_const::init    cosmictiger/ewald_indices.hpp:32-41, src/ewald_indices.cu:30-114
- *   drift with lightcone src/drift.cu:35-198 (do_lc), src/healpix.cu:55-171, lc_add_parts input
+ *   drift with lightcone src/drift.cu:35-195 (do_lc), src/healpix.cu:55-171, lc_add_parts input
  *   initialize           src/initialize.cpp:261-355 (Zel'dovich / 2LPT from power.init)
  *   power spectrum       src/power.cpp:33-77, src/power.cu:32-85, src/fft.cpp:172-360
  */
@@ -173,7 +173,7 @@ ct_status ct_tree_create(ct_ctx* ctx, int box_id, const ct_tree_params* params, 
 ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* result);
 ct_status ct_drift(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag);
 
-/* ---- drift with the lightcone capture of cuda_drift (src/drift.cu:35-198) */
+/* ---- drift with the lightcone capture of cuda_drift (src/drift.cu:35-195) */
 
 /* One crossing of the light cone (lc_entry, cosmictiger/lightcone.hpp:54-58): the crossing point
  * relative to the observer at the origin, fixed<int,31> (2^-31 box units, in [-1, 1]); the

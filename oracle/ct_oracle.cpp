@@ -192,6 +192,7 @@ struct Builder {
 	int max_nodes;
 	int count;
 	bool overflow;
+	bool too_deep;  // a node at depth MAX_DEPTH - 1 still had to split (tree.cpp:285-286)
 };
 
 // Two-pointer partition of [b, e) at xmid along xdim (particles.cpp:979-1018).
@@ -239,10 +240,11 @@ BuildRet tree_create(Builder& B, uint64_t key, int pb, int pe, const double* box
 	double Xc[3];
 	float radius;
 	bool isleaf = true;
-	if (depth >= 127) {
-		B.overflow = true;
+	const bool must_split = nparts > B.bucket || (!ewald_satisfied && nparts > 0);
+	if (must_split && depth >= 127) {
+		B.too_deep = true;
 	}
-	if (!B.overflow && (nparts > B.bucket || (!ewald_satisfied && nparts > 0))) {
+	if (!B.overflow && !B.too_deep && must_split) {
 		isleaf = false;
 		int xdim = 0;
 		double max_span = -1.0;
@@ -1106,11 +1108,15 @@ int ct_or_tree_build(int order, int n, int begin, uint32_t* x, uint32_t* y, uint
 	B.max_nodes = max_nodes;
 	B.count = 0;
 	B.overflow = false;
+	B.too_deep = false;
 	const double bb[3] = { 0, 0, 0 }, be[3] = { 1, 1, 1 };
 	if (order == 5) {
 		tree_create<Ops5>(B, 1, begin, n, bb, be, 0);
 	} else {
 		tree_create<Ops7>(B, 1, begin, n, bb, be, 0);
+	}
+	if (B.too_deep) {
+		return -2;
 	}
 	if (B.overflow) {
 		return -1;
@@ -1239,7 +1245,7 @@ static int32_t fixed31_from_double(double x) {
 
 int64_t ct_or_drift_lc(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt,
 		double drag, float tau0, float tau1, float tau_max, int nside, ct_or_lc_entry* out, int64_t max_out) {
-	// kernel arguments as cuda_drift passes them (src/drift.cu:156-197): floats widened to double
+	// kernel arguments as cuda_drift passes them (src/drift.cu:156-195): floats widened to double
 	const double da = a, ddt = dt, t0 = tau0, t1 = tau1, tmax = tau_max;
 	const bool do_lc = tmax - t1 < 1.0;
 	const double c0 = 1.0 / tmax;

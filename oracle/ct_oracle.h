@@ -70,7 +70,9 @@ typedef struct {
 } ct_or_node;
 
 /* Build the tree over particles [begin, n) in place (reorders x,y,z,v,rung exactly as the
- * reference's partition does).  Returns the node count, or -1 if max_nodes is too small. */
+ * reference's partition does).  Returns the node count, -1 if max_nodes is too small, or -2
+ * if a node at depth 127 still had to split (more than a bucket of coincident particles), where
+ * the reference throws "Maximum depth exceeded" (tree.cpp:285-286, MAX_DEPTH 128). */
 int ct_or_tree_build(int order, int n, int begin, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, double theta, double hsoft,
 		int bucket, ct_or_node* nodes, int max_nodes);
 

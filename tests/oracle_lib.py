@@ -111,6 +111,8 @@ class Oracle:
                 ctypes.c_double(theta), ctypes.c_double(hsoft), ctypes.c_int(bucket), _p(nodes), ctypes.c_int(max_nodes))
             if cnt >= 0:
                 return nodes[:cnt]
+            if cnt == -2:
+                raise RuntimeError("oracle tree build: maximum depth exceeded")
             max_nodes *= 2
             if max_nodes > 1 << 28:
                 raise RuntimeError("oracle tree build failed")
