@@ -129,7 +129,7 @@ struct PowerTable {
 // ---------------------------------------------------------------- k-space fields
 // The Gaussian field for the displacement derivatives dim1, dim2 (3: none):
 // Y(k) = n(k) sqrt(P(|k|)) box^-1.5 N^3 (-i k_dim1)(-i k_dim2) / k^2, n a unit complex normal,
-// times the cloud kernel's inverse window (twolpt_generate, initialize.cpp:416-535).  Every
+// times the cloud kernel's inverse window (twolpt_generate, initialize.cpp:436-540).  Every
 // (x, y) row of k-space has its own generator (seed (I0 N + I1) 1234 + 42, eight draws
 // discarded) for kz > 0; the kz = 0 element takes the generator of the mirrored row and its
 // conjugate on the lower half, which makes the kz = 0 plane Hermitian.  The seeds do not depend
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(FT_TPB) k_ic_field(int N, float box_size, int 
 
 // Second-order displacement field of axis dim from the transformed 2LPT source:
 // Y = -i k_dim delta2(k) / k^2 times the inverse window, 0 at k = 0 (twolpt_correction2,
-// initialize.cpp:384-430).
+// initialize.cpp:384-434).
 __global__ void __launch_bounds__(FT_TPB) k_ic_correction(const cufftComplex* __restrict__ src, cufftComplex* __restrict__ Y, int N, float box_size, int dim) {
 	const int NZ = N / 2 + 1;
 	const int64_t total = (int64_t) N * N * NZ;
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(FT_TPB) k_ic_correction(const cufftComplex* __
 }
 
 // ---------------------------------------------------------------- real space
-// The lattice (init_X0, initialize.cpp:646-690): particle (I0 N + I1) N + I2 at I / N, at rest,
+// The lattice (init_X0, initialize.cpp:650-798): particle (I0 N + I1) N + I2 at I / N, at rest,
 // rung 0.
 __global__ void __launch_bounds__(FT_TPB) k_ic_lattice(int N, uint32_t* __restrict__ x, uint32_t* __restrict__ y, uint32_t* __restrict__ z,
 		float* __restrict__ v0, float* __restrict__ v1, float* __restrict__ v2, int8_t* __restrict__ rung) {
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(FT_TPB) k_ic_lattice(int N, uint32_t* __restri
 	}
 }
 
-// Displacement of axis dim (zeldovich_end, initialize.cpp:786-851): the field interpolated
+// Displacement of axis dim (zeldovich_end, initialize.cpp:800-868): the field interpolated
 // with the cloud kernel at each particle's lattice point, dx = -D field / box; the position
 // moves by dx (periodic) and the velocity by prefac dx.  Particle (I0 N + I1) N + I2 sits at
 // lattice point I, and the kernel's 6^3 weights there are products of per-axis weights that
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(FT_TPB) k_ic_displace(int N, const double* __r
 	}
 }
 
-// The 2LPT source (twolpt_phase, initialize.cpp:562-583): phases 0..8 bring the second
+// The 2LPT source (twolpt_phase, initialize.cpp:565-589): phases 0..8 bring the second
 // derivatives (yy, zz, xx, zz, xx, yy, xy, xz, yz); an even phase up to 6 keeps its field, an
 // odd one adds the product with the kept field, and phases 7 and 8 subtract their squares:
 // delta2 = p_yy p_zz + p_xx p_zz + p_xx p_yy - p_xz^2 - p_yz^2 (the reference keeps p_xy at
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(FT_TPB) k_density(int64_t n, const uint32_t* _
 	}
 }
 
-// Bin of |k| (grid units) among the log-spaced edges (search_kbins, fft.cpp:216-238): -1 below
+// Bin of |k| (grid units) among the log-spaced edges (search_kbins, fft.cpp:219-237): -1 below
 // 0 or at / above the last edge.
 __device__ __forceinline__ int k_bin(const float* kb, int nb, double k) {
 	if (k < 0.0 || k >= kb[nb]) {
@@ -565,7 +565,7 @@ double growth_factor(double omega_m, float a) {
 }
 
 // sigma8 normalisation of the table (power_spectrum_function::normalize and
-// sigma8_integrand, initialize.cpp:140-173): Simpson's rule over 8192 log-k intervals of the
+// sigma8_integrand, initialize.cpp:141-172): Simpson's rule over 8192 log-k intervals of the
 // top-hat variance at R = 8 / h Mpc, in float; the table is scaled in place and the factor
 // returned.
 float sigma8_normalize(PowerTable& t, std::vector<float>& P, float logkmax_table, double hubble, double sigma8) {
@@ -622,7 +622,7 @@ extern "C" ct_status ct_initialize(ct_ctx* ctx, int box_id, const ct_ic_params* 
 			!(p->z0 > -1.0)) {
 		return fail(c, CT_ERR_ARG, "ct_initialize: bad parameters or power table");
 	}
-	// the table as read_power_spectrum takes it (initialize.cpp:853-880): k h / Mpc -> 1 / Mpc,
+	// the table as read_power_spectrum takes it (initialize.cpp:870-898): k h / Mpc -> 1 / Mpc,
 	// P (Mpc / h)^3 -> Mpc^3, log-uniform in k
 	const float h = (float) p->hubble;
 	std::vector<float> P(p->ntable);

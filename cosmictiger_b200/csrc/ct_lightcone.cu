@@ -1,4 +1,4 @@
-// Drift with the lightcone capture of the reference's cuda_drift_kernel (src/drift.cu:35-154).
+// Drift with the lightcone capture of the reference's cuda_drift_kernel (src/drift.cu:36-154).
 //
 // The rung's particles move as k_drift moves them (the FP64 update, wrap and fixed32 store),
 // and each crossing of the light cone in the 8 periodic images next to the observer is

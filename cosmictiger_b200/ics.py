@@ -127,7 +127,7 @@ def eta_default(eta=0.25):
 
 def read_power_init(path):
     """The rows of a power.init file (two columns: k in h/Mpc, P in (Mpc/h)^3; the format
-    read_power_spectrum reads, src/initialize.cpp:853-880), as float32 arrays."""
+    read_power_spectrum reads, src/initialize.cpp:870-898), as float32 arrays."""
     rows = np.loadtxt(path, dtype=np.float64, ndmin=2)
     return rows[:, 0].astype(np.float32), rows[:, 1].astype(np.float32)
 

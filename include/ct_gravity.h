@@ -15,7 +15,7 @@
  *                        src/kick.cu:179-609 (cuda_execute_kicks)
  *   drift                cosmictiger/drift.hpp:51-54, src/drift.cu:36-185
  *   ewald_const::init    cosmictiger/ewald_indices.hpp:32-41, src/ewald_indices.cu:30-114
- *   drift with lightcone src/drift.cu:35-195 (do_lc), src/healpix.cu:55-171, lc_add_parts input
+ *   drift with lightcone src/drift.cu:36-195 (do_lc), src/healpix.cu:55-171, lc_add_parts input
  *   initialize           src/initialize.cpp:261-355 (Zel'dovich / 2LPT from power.init)
  *   power spectrum       src/power.cpp:33-77, src/power.cu:32-85, src/fft.cpp:172-360
  */
@@ -173,7 +173,7 @@ ct_status ct_tree_create(ct_ctx* ctx, int box_id, const ct_tree_params* params, 
 ct_status ct_kick(ct_ctx* ctx, int box_id, const ct_kick_params* params, ct_kick_return* result);
 ct_status ct_drift(ct_ctx* ctx, int box_id, int rung, float a, float dt, double drag);
 
-/* ---- drift with the lightcone capture of cuda_drift (src/drift.cu:35-195) */
+/* ---- drift with the lightcone capture of cuda_drift (src/drift.cu:36-195) */
 
 /* One crossing of the light cone (lc_entry, cosmictiger/lightcone.hpp:54-58): the crossing point
  * relative to the observer at the origin, fixed<int,31> (2^-31 box units, in [-1, 1]); the
@@ -222,7 +222,7 @@ typedef struct {
 	double sigma8;          /* normalisation of the table */
 	double H0;              /* Hubble constant in code time units (constants::H0 code_to_s h) */
 	int twolpt;             /* add the second-order displacements */
-	const float* table_k;   /* power.init rows (read_power_spectrum, initialize.cpp:853-880): */
+	const float* table_k;   /* power.init rows (read_power_spectrum, initialize.cpp:870-898): */
 	const float* table_p;   /*   k in h / Mpc, log-uniform; P in (Mpc / h)^3 */
 	int ntable;
 } ct_ic_params;
@@ -282,7 +282,7 @@ ct_status ct_step_hierarchical(ct_ctx* ctx, int box_id, const ct_step_params* pa
 /* The active-range state of the hierarchical rung ladder: the start of the active range
  * (particles_current_range) and the saved starts of the enclosing ranges, innermost last
  * (particles_push/pop_rungs, src/particles.cpp:218-235) -- what particles_save writes after
- * the particles (src/particles.cpp:1216-1219), so that a run resumes where it stopped.
+ * the particles (src/particles.cpp:1220-1223), so that a run resumes where it stopped.
  * get: pass stack = NULL to learn the depth; set: restores both (begin <= box size). */
 ct_status ct_box_get_rung_state(ct_ctx* ctx, int box_id, int64_t* rung_begin, int64_t* stack, int* depth);
 ct_status ct_box_set_rung_state(ct_ctx* ctx, int box_id, int64_t rung_begin, const int64_t* stack, int depth);

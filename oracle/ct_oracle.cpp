@@ -49,7 +49,7 @@ constexpr double FIXED2DOUBLE = 1.0 / 4294967296.0;
 inline uint32_t fixed32_from_double(double x) {
 	return (uint32_t) (int64_t) (x * 4294967296.0);
 }
-// fixed<int,29> from double (range.hpp:356; fixed.hpp:97-101).
+// fixed<int,29> from double (range.hpp:358; fixed.hpp:97-101).
 inline int32_t range_fixed_from_double(double x) {
 	return (int32_t) (x * 536870912.0);
 }

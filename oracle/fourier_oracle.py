@@ -69,7 +69,7 @@ def cloud_filter(kh):
 # ---------------------------------------------------------------- power table
 def power_table(table_k, table_p, hubble, sigma8):
     """(P in Mpc^3, logkmin, dlogk, logkmax, norm) as read_power_spectrum + normalize take the
-    table (initialize.cpp:140-173,853-880), in double."""
+    table (initialize.cpp:141-172,853-880), in double."""
     k = np.asarray(table_k, np.float64) * hubble
     P = np.asarray(table_p, np.float64) / hubble ** 3
     logkmin, logkmax = np.log(k.min()), np.log(k.max())
@@ -112,7 +112,7 @@ def interp_power(P, logkmin, dlogk, k):
 
 # ---------------------------------------------------------------- fields
 def modes(N, box, dim1, dim2, P, logkmin, dlogk):
-    """The half-complex field Y[I0, I1, I2] of twolpt_generate (initialize.cpp:416-535)."""
+    """The half-complex field Y[I0, I1, I2] of twolpt_generate (initialize.cpp:436-540)."""
     NZ = N // 2 + 1
     I0, I1 = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
     I0, I1 = I0.ravel(), I1.ravel()

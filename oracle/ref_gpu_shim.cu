@@ -95,7 +95,7 @@ void cosmictiger_assert(const char* cond, bool ok, const char* file, int line) {
 	}
 }
 
-// Where cuda_drift hands its per-block lightcone lists over (src/drift.cu:193): the harness
+// Where cuda_drift hands its per-block lightcone lists over (src/drift.cu:188): the harness
 // collects the entries (the lists live in the reference's managed heap, readable here after
 // the drift's synchronisation) instead of binning them into HEALPix maps and files.
 static std::vector<lc_entry> g_lc;
@@ -358,7 +358,7 @@ int ctref_drift(int64_t n, int64_t rung_begin, uint32_t* x, uint32_t* y, uint32_
 }
 
 // The reference's drift with its lightcone capture on (options do_lc, lc_map_size = nside;
-// create_glass selects its drag of pi, src/drift.cu:182): particles as in ctref_drift, the
+// create_glass selects its drag of pi, src/drift.cu:183): particles as in ctref_drift, the
 // velocities written back (the drag changes them), and the recorded entries copied to out
 // (at most max_out; *nout receives how many there were).  healpix_init fills the pixel tables
 // of vec2pix_nest as the reference's start-up does.

@@ -87,7 +87,7 @@ def test_displacements_first_order_dominate_with_a_cut_spectrum():
 
 def test_sigma8_normalisation_by_independent_quadrature():
     """The normalised table's top-hat variance at R = 8/h Mpc, integrated by adaptive quadrature
-    over the same k range, is sigma8^2 (the restated Simpson sum, initialize.cpp:140-173)."""
+    over the same k range, is sigma8^2 (the restated Simpson sum, initialize.cpp:141-172)."""
     from scipy import integrate
 
     k, P = ics.power_law_table()

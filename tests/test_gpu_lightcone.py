@@ -66,7 +66,7 @@ def test_lightcone_matches_reference_cuda_drift(ctx, ref, level, a, dt, tau0, ta
     velocities as the reference's drift with its lightcone on, bit for bit."""
     st = _state(vscale=vscale)
     tau1 = tau0 + dt
-    drag = np.pi if glass else 0.0  # the reference's drift takes pi with create_glass (drift.cu:182)
+    drag = np.pi if glass else 0.0  # the reference's drift takes pi with create_glass (drift.cu:183)
     out, ent = _drift(ctx, st, level, a, dt, tau0, tau1, tau_max, nside, drag)
     rx, ry, rz, rv, rent = ref.drift_lc(*st, level, a, dt, tau0, tau1, tau_max, nside, create_glass=glass)
     print("lightcone vs reference CUDA drift: %d entries, %d particles of rung %d" % (len(rent), int(np.sum(st[4] == level)), level))

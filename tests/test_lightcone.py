@@ -1,4 +1,4 @@
-"""Lightcone capture in the drift (src/drift.cu:35-154) and its HEALPix pixels
+"""Lightcone capture in the drift (src/drift.cu:36-154) and its HEALPix pixels
 (src/healpix.cu:55-171): properties of the CPU oracle's restatement.  The CUDA path is checked
 against the reference's own drift kernel and against this oracle in test_gpu_lightcone.py."""
 import numpy as np
