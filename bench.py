@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256, help="particles = n^3")
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=256, help="particles = n^3 (spell it --grid under torch.distributed.run, which takes --n for its own --nnodes/--nproc-per-node)")
     ap.add_argument("--theta", type=float, default=0.55)
     ap.add_argument("--workload", default="clustered", choices=["clustered", "lattice"])
     ap.add_argument("--mode", default="multistep", choices=["multistep", "single"],

@@ -40,3 +40,23 @@ def test_read_power_init_round_trip(tmp_path):
     # log-uniform in k, as the reference's reader assumes
     d = np.diff(np.log(k2.astype(np.float64)))
     assert np.allclose(d, d[0], rtol=1e-4)
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    """Launched as the multi-GPU bench is (torch.distributed.run, two ranks on one node): rank 0
+    alone runs the CPU reference arm and prints the one JSON line; the other rank exits 0
+    without work."""
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+           "--master-port", str(port), os.path.join(ROOT, "bench.py"), "--impl", "reference", "--grid", "32", "--steps", "1", "--warmup", "0"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.lstrip().startswith("{")]
+    assert len(lines) == 1, out.stdout[-2000:]
+    d = json.loads(lines[0].strip())
+    assert d["impl"] == "reference" and d["value"] > 0
