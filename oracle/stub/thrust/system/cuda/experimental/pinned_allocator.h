@@ -1,4 +1,4 @@
-// Stand-in for a Thrust header that current CCCL no longer ships; the reference's
+// Test infrastructure only (oracle build). Stand-in for a Thrust header that current CCCL no longer ships; the reference's
 // cosmictiger/cuda.hpp includes it only for a pinned-allocator alias.
 #pragma once
 #include <memory>
