@@ -294,8 +294,6 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     # events on the library's own stream
-    ctx.lib.ct_stream.argtypes = [ctypes.c_void_p]
-    ctx.lib.ct_stream.restype = ctypes.c_void_p
     lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
     torch.cuda.synchronize()
     if pg:
@@ -420,7 +418,6 @@ def main():
         multistep["single_rung_ms_per_step"] = e0s.elapsed_time(e1s) / ks
     # ---- roofline of the leaf kernel (reference flop convention)
     L = ctx.lib
-    L.ct_fp32_peak.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
     pk = ctypes.c_double(0)
     ctx.check(L.ct_fp32_peak(ctx.h, ctypes.byref(pk)), "ct_fp32_peak")
     peak_tf = pk.value

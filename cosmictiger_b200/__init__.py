@@ -186,6 +186,11 @@ def library():
     L.ct_rung_counts.argtypes = [vp, i32, vp]
     L.ct_launch_count.argtypes = [vp]
     L.ct_launch_count.restype = ctypes.c_ulonglong
+    L.ct_order.argtypes = [vp]
+    L.ct_stream.argtypes = [vp]
+    L.ct_stream.restype = vp  # a cudaStream_t: a 64-bit handle, not an int
+    L.ct_fp32_peak.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.ct_sort_by_rung_noalloc.argtypes = [i64, i64, i32, vp, vp, vp, vp, vp, vp, vp, ctypes.POINTER(i64), vp]
     L.ct_direct_ewald.argtypes = [vp, i32, i64, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
     L.ct_drift_lightcone.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_double, ctypes.POINTER(LcParams), ctypes.POINTER(i64)]
     L.ct_lightcone_count.argtypes = [vp, i32, ctypes.POINTER(i64)]

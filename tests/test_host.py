@@ -109,3 +109,35 @@ def test_ics_fixed_point_and_shapes():
     cx, cy, cz, cv, cr = ics.clustered_box(16, nspheres=20, seed=2)
     assert len(cx) == 16 ** 3
     assert ics.to_fixed32(np.array([0.0, 0.5, 1.0 - 1e-12, -0.25]))[1] == 2 ** 31
+
+
+def _header_prototypes():
+    """name -> number of parameters of every function declared in include/ct_gravity.h."""
+    src = open(os.path.join(ROOT, "include", "ct_gravity.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(ct_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", src):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_bindings_match_the_header():
+    """Every function the header declares has an argtypes list in the Python binding with as many
+    entries as the C prototype has parameters (a mismatch, or a missing list, would pass
+    truncated or shifted values through the ABI without an error)."""
+    import cosmictiger_b200 as ct
+
+    L = ct.library()
+    protos = _header_prototypes()
+    assert len(protos) >= 40
+    for name, nparams in protos.items():
+        fn = getattr(L, name)
+        assert fn.argtypes is not None, name
+        assert len(fn.argtypes) == nparams, (name, len(fn.argtypes), nparams)
+    # returns wider than int keep their width (ctypes' default restype is a 32-bit int)
+    import ctypes
+
+    for name, rt in (("ct_stream", ctypes.c_void_p), ("ct_last_error", ctypes.c_char_p), ("ct_launch_count", ctypes.c_ulonglong)):
+        assert getattr(L, name).restype is rt, name
+    assert ctypes.sizeof(L.ct_box_size.restype) == 8 and ctypes.sizeof(L.ct_bytes_in_use.restype) == 8
