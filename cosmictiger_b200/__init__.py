@@ -244,6 +244,21 @@ class Context:
     def synchronize(self):
         self.check(self.lib.ct_synchronize(self.h), "ct_synchronize")
 
+    def stream_handle(self):
+        """The context's cudaStream_t as an integer (ct_stream), e.g. for
+        torch.cuda.ExternalStream, to order other work or events with the library's."""
+        return int(self.lib.ct_stream(self.h) or 0)
+
+    def fp32_peak(self):
+        """Measured FP32 FMA throughput of the device, TFLOP/s (ct_fp32_peak)."""
+        pk = ctypes.c_double(0)
+        self.check(self.lib.ct_fp32_peak(self.h, ctypes.byref(pk)), "ct_fp32_peak")
+        return pk.value
+
+    def device_order(self):
+        """Expansion order the context was created with (ct_order)."""
+        return int(self.lib.ct_order(self.h))
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.ct_ctx_destroy(self.h)
@@ -338,6 +353,20 @@ class Box:
     def upload_device(self, x, y, z, vxyz, rung):
         """Device pointers (e.g. torch tensor data_ptr()) with the same layout."""
         self.ctx.check(self.ctx.lib.ct_box_upload_device(self.ctx.h, self.id, *[_p(a) for a in (x, y, z, vxyz, rung)]), "ct_box_upload_device")
+
+    def download_device(self, x, y, z, vxyz, rung, gx=None, gy=None, gz=None, pot=None):
+        """Copy the box's particles into device buffers the caller holds (data_ptr() integers or
+        None to skip a field); gx..pot only after a kick with save_force."""
+        ptrs = [_p(a) for a in (x, y, z, vxyz, rung, gx, gy, gz, pot)]
+        self.ctx.check(self.ctx.lib.ct_box_download_device(self.ctx.h, self.id, *ptrs), "ct_box_download_device")
+
+    def size(self):
+        """Particles held by the box (ct_box_size)."""
+        return int(self.ctx.lib.ct_box_size(self.ctx.h, self.id))
+
+    def box_count(self):
+        """Boxes in an ensemble, 1 for a plain box (ct_box_count)."""
+        return int(self.ctx.lib.ct_box_count(self.ctx.h, self.id))
 
     def download(self, forces=False):
         n = self.n
