@@ -141,3 +141,33 @@ def test_ctypes_bindings_match_the_header():
     for name, rt in (("ct_stream", ctypes.c_void_p), ("ct_last_error", ctypes.c_char_p), ("ct_launch_count", ctypes.c_ulonglong)):
         assert getattr(L, name).restype is rt, name
     assert ctypes.sizeof(L.ct_box_size.restype) == 8 and ctypes.sizeof(L.ct_bytes_in_use.restype) == 8
+
+
+_NULL_CTX = r'''
+import ctypes, sys
+sys.path.insert(0, %r)
+import cosmictiger_b200 as ct
+L = ct.library()
+numbers = (ctypes.c_int, ctypes.c_int64, ctypes.c_float, ctypes.c_double, ctypes.c_size_t, ctypes.c_ulonglong)
+for name in %r:
+    fn = getattr(L, name)
+    r = fn(*[0 if t in numbers else None for t in fn.argtypes])
+    print(name, r, flush=True)
+'''
+
+
+def test_entry_points_reject_a_null_context():
+    """Every ct_status entry point taking a context returns an error for a NULL context and null
+    arguments instead of dereferencing them (run in a child process, so that a crash is a test
+    failure rather than the end of the test run).  No device is touched."""
+    import cosmictiger_b200 as ct
+
+    ct.library()
+    src = open(os.path.join(ROOT, "include", "ct_gravity.h")).read()
+    names = sorted(n for n in _header_prototypes() if re.search(r"ct_status\s+" + n + r"\s*\(\s*ct_ctx\s*\*", src) and n != "ct_ctx_create")
+    assert len(names) >= 30
+    out = subprocess.run([sys.executable, "-c", _NULL_CTX % (ROOT, names)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr[-2000:]
+    got = dict(ln.split() for ln in out.stdout.splitlines())
+    assert sorted(got) == names
+    assert all(int(v) < 0 for v in got.values()), got
