@@ -1,5 +1,5 @@
 // Fourier-space work around the gravity step: the reference's initial-condition generator
-// (Zel'dovich and 2LPT displacements of a lattice, src/initialize.cpp:261-355,416-868) and its
+// (Zel'dovich and 2LPT displacements of a lattice, src/initialize.cpp:261-355,436-898) and its
 // matter power spectrum (src/power.cpp:33-77, src/power.cu:32-85, src/fft.cpp:172-330).
 //
 // Both follow the reference's conventions: grids of Nfour^3 points in x-major order, the

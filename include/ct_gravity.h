@@ -212,7 +212,7 @@ ct_status ct_lightcone_download(ct_ctx* ctx, int box_id, ct_lc_entry* out, int64
 ct_status ct_lightcone_reserve(ct_ctx* ctx, int box_id, int64_t entries);
 
 /* ---- initial conditions: Zel'dovich / 2LPT displacements of a lattice
- * (initialize, src/initialize.cpp:261-355; the field of twolpt_generate, :416-535) */
+ * (initialize, src/initialize.cpp:261-355; the field of twolpt_generate, :436-540) */
 typedef struct {
 	int nfour;              /* particles per dimension = FFT grid (parts_dim = Nfour), even, 4 .. 1024 */
 	double box_size;        /* box size in Mpc (code_to_cm / mpc_to_cm) */

@@ -1,5 +1,5 @@
 """Test infrastructure only: a numpy restatement of the reference's initial-condition generator
-(src/initialize.cpp:261-355,416-868) and matter power spectrum (src/power.cpp:33-77,
+(src/initialize.cpp:261-355,436-898) and matter power spectrum (src/power.cpp:33-77,
 src/power.cu:32-85, src/fft.cpp:172-360), the checker of the CUDA path (ct_initialize,
 ct_power_spectrum).  Transforms are numpy's FFTs in double precision; the random field uses the
 same per-row generator (GSL's "taus", L'Ecuyer 1996, restated below), so that both sides draw
