@@ -30,6 +30,10 @@ def tune_bucket(ctx, state, theta=0.55, h=None, candidates=(64, 96, 128, 160, 19
     (x, y, z, vxyz, rung) host arrays of one box; `max_force_rms` None skips the force check."""
     from . import KickParams
 
+    if repeats < 1:
+        raise ValueError("repeats must be >= 1 (the first run of each candidate is not timed)")
+    if not candidates:
+        raise ValueError("no candidate leaf sizes")
     x, y, z, v, r = state
     n = len(x)
     h = ics.softening(n, 0.02) if h is None else h

@@ -3,6 +3,7 @@ chosen, candidates whose forces leave the tolerance are excluded, particles are 
 position although every run returns them in another order, and the state is uploaded before
 every run."""
 import numpy as np
+import pytest
 
 from cosmictiger_b200 import autotune
 
@@ -81,3 +82,14 @@ def test_force_tolerance_excludes_candidates():
     for b, e in ERR.items():
         assert abs(errs[b] - e) < 1e-9, (b, errs[b])
     assert res["best"] == 96  # 160 is faster but changes the forces by 5e-3
+
+
+def test_rejects_untimed_settings():
+    """Every candidate's first run only grows buffers, so at least one more is needed; an empty
+    candidate list has nothing to choose.  Both are refused before any device work."""
+    ctx = FakeContext(500)
+    with pytest.raises(ValueError):
+        autotune.tune_bucket(ctx, _state(500), repeats=0)
+    with pytest.raises(ValueError):
+        autotune.tune_bucket(ctx, _state(500), candidates=())
+    assert not ctx.boxes
