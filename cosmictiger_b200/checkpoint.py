@@ -130,6 +130,10 @@ def load_box(ctx, path, **kw):
     """A new box holding a checkpoint's particles and rung-ladder state; returns (box, params)."""
     c = read_checkpoint(path, **kw)
     box = ctx.box(len(c["x"]))
-    box.upload(c["x"], c["y"], c["z"], c["v"], c["rung"])
-    box.set_rung_state(c["rung_begin"], c["rung_begins"])
+    try:
+        box.upload(c["x"], c["y"], c["z"], c["v"], c["rung"])
+        box.set_rung_state(c["rung_begin"], c["rung_begins"])
+    except Exception:
+        box.close()  # a state the library refuses (e.g. rung_begin beyond N) frees its box
+        raise
     return box, c["params"]

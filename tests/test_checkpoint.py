@@ -119,3 +119,34 @@ def test_layouts_match_the_reference_compiler():
     lc = ct.LC_ENTRY
     assert lc.itemsize == ref["lc_entry"]["size"]
     assert lc.fields["vx"][1] == ref["lc_entry"]["vx"] and lc.fields["pix"][1] == ref["lc_entry"]["pix"]
+
+
+def test_load_box_frees_the_box_when_the_state_is_refused(tmp_path):
+    """A checkpoint whose rung state the library refuses leaves no box behind (a fake context
+    stands in for the device)."""
+
+    class FakeBox:
+        closed = False
+
+        def upload(self, *a):
+            pass
+
+        def set_rung_state(self, rung_begin, stack):
+            raise RuntimeError("rung_begin beyond the box")
+
+        def close(self):
+            self.closed = True
+
+    class FakeCtx:
+        def box(self, n):
+            self.made = FakeBox()
+            return self.made
+
+    n = 8
+    x = np.arange(n, dtype=np.uint32)
+    path = str(tmp_path / "bad.chk")
+    ck.write_checkpoint(path, ck.default_params(a=1.0), x, x, x, np.zeros((n, 3), np.float32), np.zeros(n, np.int8), rung_begin=99)
+    ctx = FakeCtx()
+    with pytest.raises(RuntimeError):
+        ck.load_box(ctx, path)
+    assert ctx.made.closed
