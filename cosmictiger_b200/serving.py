@@ -166,18 +166,21 @@ class Server:
         pending = sorted(requests, key=lambda r: r.arrival)
         t_start = clock()
         now = lambda: clock() - t_start  # noqa: E731
-        while pending or self.waiting or self.active:
-            t = now()
-            while pending and pending[0].arrival <= t:
-                self.waiting.append(pending.pop(0))
-            self.admit(t, states)
-            if self.active:
-                self.tick(now)
-            elif pending:
-                time.sleep(max(0.0, min(0.01, pending[0].arrival - now())))
-        if self.ens is not None:
-            self.ens.close()
-            self.ens = None
+        try:
+            while pending or self.waiting or self.active:
+                t = now()
+                while pending and pending[0].arrival <= t:
+                    self.waiting.append(pending.pop(0))
+                self.admit(t, states)
+                if self.active:
+                    self.tick(now)
+                elif pending:
+                    time.sleep(max(0.0, min(0.01, pending[0].arrival - now())))
+        finally:
+            # also when a step raises: the ensemble's device arrays go back to the context
+            if self.ens is not None:
+                self.ens.close()
+                self.ens = None
         return self.finished
 
 
