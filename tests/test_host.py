@@ -171,3 +171,46 @@ def test_entry_points_reject_a_null_context():
     got = dict(ln.split() for ln in out.stdout.splitlines())
     assert sorted(got) == names
     assert all(int(v) < 0 for v in got.values()), got
+
+
+_ABI_PROGRAM = r'''
+#include <stdio.h>
+#include "ct_gravity.h"
+int main(void) {
+	ct_ctx* ctx = NULL;
+	ct_status s = ct_ctx_create(&ctx, 0, 0, 7);
+	if (s == CT_OK) {
+		printf("context order %d\n", ct_order(ctx));
+		ct_ctx_destroy(ctx);
+		return 0;
+	}
+	printf("status %d\n", (int) s);
+	return s < 0 ? 0 : 1;
+}
+'''
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c99"), ("g++", "-std=c++17")])
+def test_header_compiles_and_links_from_c_and_cpp(tmp_path, compiler, std):
+    """include/ct_gravity.h is plain C (and C++): a program written against it alone compiles
+    with warnings as errors, links against libct_gravity.so and runs; without a device the
+    context call returns an error status instead of failing."""
+    import shutil
+
+    from cosmictiger_b200 import LIB_PATH, build
+
+    if shutil.which(compiler) is None:
+        pytest.skip(compiler + " not installed")
+    if not os.path.exists(LIB_PATH):
+        build.build()
+    src = tmp_path / ("abi.c" if compiler == "gcc" else "abi.cpp")
+    src.write_text(_ABI_PROGRAM)
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(LIB_PATH)
+    cmd = [compiler, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-I" + os.path.join(ROOT, "include"), str(src), "-L" + libdir, "-lct_gravity",
+           "-Wl,-rpath," + libdir, "-o", str(exe)]
+    cc = subprocess.run(cmd, capture_output=True, text=True, timeout=120)
+    assert cc.returncode == 0, cc.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert run.stdout.startswith(("context order 7", "status -")), run.stdout
