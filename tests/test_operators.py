@@ -105,3 +105,18 @@ def full_exponents(P):
             for b in range(N - a, -1, -1):
                 out.append((a, b, N - a - b))
     return out
+
+
+@pytest.mark.parametrize("order", [7, 5])
+def test_generated_operator_headers_are_current(order):
+    """The committed operator headers (csrc/fmm_p{7,5}.h, compiled into both the library and the
+    oracle) are exactly what csrc/gen_fmm.py generates, so an edit of the generator cannot
+    leave the two behind each other."""
+    import importlib.util
+
+    csrc = os.path.join(os.path.dirname(HERE), "cosmictiger_b200", "csrc")
+    spec = importlib.util.spec_from_file_location("gen_fmm", os.path.join(csrc, "gen_fmm.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    with open(os.path.join(csrc, "fmm_p%d.h" % order)) as f:
+        assert f.read() == gen.gen_header(order)
