@@ -150,3 +150,21 @@ def test_load_box_frees_the_box_when_the_state_is_refused(tmp_path):
     with pytest.raises(RuntimeError):
         ck.load_box(ctx, path)
     assert ctx.made.closed
+
+
+@pytest.mark.parametrize("probe,fixture", [("layout_probe", "ref_layouts.json"), ("func_probe", "ref_functions.json")])
+def test_reference_fixtures_equal_their_probes(probe, fixture):
+    """Where the probes built from the reference's sources are present (oracle/_ref, made by
+    `make -C oracle layout funcs`), their output equals the committed fixture byte for byte, so
+    the fixtures cannot drift from the reference they were recorded from."""
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "oracle", "_ref", probe)
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/%s not built (needs the reference's sources)" % probe)
+    out = subprocess.run([exe], capture_output=True, timeout=60)
+    assert out.returncode == 0
+    with open(os.path.join(root, "tests", "golden", fixture), "rb") as f:
+        assert out.stdout == f.read()
