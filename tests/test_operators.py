@@ -120,3 +120,22 @@ def test_generated_operator_headers_are_current(order):
     spec.loader.exec_module(gen)
     with open(os.path.join(csrc, "fmm_p%d.h" % order)) as f:
         assert f.read() == gen.gen_header(order)
+
+
+@pytest.mark.parametrize("order", [7, 5])
+def test_operator_goldens_equal_a_fresh_recording(order):
+    """Where the reference's operators are built (oracle/_ref/libctref_p{7,5}.so, from
+    `make -C oracle ref`), recording the golden vectors again gives the committed files exactly."""
+    import importlib.util
+
+    root = os.path.dirname(HERE)
+    if not os.path.exists(os.path.join(root, "oracle", "_ref", "libctref_p%d.so" % order)):
+        pytest.skip("reference operators not built")
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(HERE, "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    fresh = mg.vectors(order)
+    g = golden(order)
+    assert sorted(fresh) == sorted(g.files)
+    for k in g.files:
+        assert np.array_equal(fresh[k], g[k]), k
