@@ -138,4 +138,10 @@ def test_operator_goldens_equal_a_fresh_recording(order):
     g = golden(order)
     assert sorted(fresh) == sorted(g.files)
     for k in g.files:
-        assert np.array_equal(fresh[k], g[k]), k
+        a, b = fresh[k], g[k]
+        if k.startswith("l2p_"):
+            # the reference's L2P writes four of its five outputs (potential and force); the
+            # fifth is whatever the harness's stack held, so only the four are compared, here
+            # as in the parity test above
+            a, b = a[:, :4], b[:, :4]
+        assert np.array_equal(a, b), k
