@@ -261,6 +261,7 @@ def main():
         return kr
 
     ms = None
+    cpu_seed = ((x, y, z, v, r), None, t0)
     if args.mode == "multistep":
         # choose t0 so that the rung rule dt = eta sqrt(a h / |g|) (kick.cu:133-136) spreads the
         # particles over rungs 0-3: 1% of them want rung >= 3
@@ -270,6 +271,9 @@ def main():
         gm = np.sqrt(g["gx"].astype(np.float64) ** 2 + g["gy"] ** 2 + g["gz"] ** 2)
         dts = eta * np.sqrt(h / np.maximum(gm, 1e-30))
         ms = {"t0": float(8.0 * np.percentile(dts, 1))}
+        # the CPU legs start from these particles (tree order) with rungs set by these forces
+        cpu_seed = ((g["x"], g["y"], g["z"], g["v"], g["rung"]), np.stack([g["gx"], g["gy"], g["gz"]], 1), ms["t0"])
+        del g, gm, dts
         box.upload(x, y, z, v, r)
         box.sort_by_rung(0)
         ms["state"] = dict(minrung=0, max_rung=0, tau=0.0)
@@ -378,7 +382,7 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(lib_stream)
-        ke = max(1, min(args.steps, 3))
+        ke = args.steps
         for i in range(ke):
             e2e_step(False)
         e1.record(lib_stream)
@@ -444,8 +448,15 @@ def main():
         # below for another's check
         acc = accuracy(box, args.accuracy_sinks, h, N)
     cpu = None
+    c1 = None
     if not args.no_cpu and rank == 0 and world == 1:
-        cpu = cpu_baseline(args)
+        cpu = cpu_baseline(args, *cpu_seed)
+        try:
+            c1 = {"workload": "lattice 64^3 Zel'dovich k^-2, 0.25 spacing RMS, theta 0.7, order 7, Ewald, one all-particles step (tree, kick, drift)",
+                  "gpu": gpu_c1(ct, torch, ctx, lib_stream), "cpu_full": cpu_c1_full()}
+            c1["e2e_speedup"] = c1["cpu_full"]["seconds"] * 1e3 / c1["gpu"]["e2e_ms"]
+        except Exception as e:  # reported, never required
+            c1 = {"failed": str(e)}
     if pg:
         pg.barrier()
     if rank == 0:
@@ -478,6 +489,8 @@ def main():
             line["ensemble"] = ens_res
         if multistep:
             line["multistep"] = multistep
+        if c1:
+            line["c1_unsampled"] = c1
         print(json.dumps(line), flush=True)
     box.close()
     ctx.close()
@@ -525,65 +538,167 @@ def accuracy(box, nsink, h, N):
                           "(rms and 99th percentile); mag = ||g|-|g_ref||/|g_ref| (the reference's force test, analytic.cpp:78-89)"}
 
 
-def cpu_measure(args, target_s=12.0, state=None):
-    """Time the CPU oracle on a bounded sample: full tree build and drift, the kick on every
-    k-th top-level work item (k chosen so the kick sample takes about target_s)."""
+def cpu_start_state(args, state, g, t0):
+    """Starting state of the CPU legs: the workload's particles (in the order `g` belongs to)
+    with the rungs the rung rule gives for the forces g (N, 3) at step t0, the active range and
+    rung stack those rungs leave (tests/oracle_lib.rung_state_from_forces), and the step
+    parameters of the benchmark's hierarchical step.  With g None (--mode single) every particle
+    stays on rung 0 and a step kicks all of them."""
     from cosmictiger_b200 import ics
     from tests import oracle_lib
 
     O = oracle_lib.load(build=False)
-    if state is None:
-        state = make_ics(args, seed=3)
-    x, y, z, v, r = (a.copy() for a in state)
+    x, y, z, v, r = state
     N = len(x)
     h = ics.softening(N, 0.02)
-    t = time.perf_counter()
-    nodes = O.tree_build(x, y, z, v, r, args.theta, h, 128)
-    t_tree = time.perf_counter() - t
-    kp = oracle_lib.KickParams(sign=1.0, min_rung=0, a=1.0, t0=1.0 / 64, theta=args.theta, h=h, eta=ics.eta_default(), GM=1.0 / N, max_dt=1e30,
-                               save_force=1, first_call=0, ascending=1, descending=1, top=1, do_phi=1)
-    ncores = os.cpu_count() or 1
-    # probe with a sparse sample, then size the real sample
-    stride = 4096
-    dt, got, _ = O.kick_sampled(kp, nodes, x, y, z, v.copy(), r.copy(), stride, nthreads=ncores)
-    rate = got / max(dt, 1e-6)
-    want = max(1, int(rate * target_s))
-    stride = max(1, int(round(N / max(want, 1))))
-    dt, got, _ = O.kick_sampled(kp, nodes, x, y, z, v.copy(), r.copy(), stride, nthreads=ncores)
-    t = time.perf_counter()
-    O.drift(x, y, z, v, r, 0, 1.0, 1.0 / 64)
-    t_drift = time.perf_counter() - t
-    t_step = t_tree + dt * (N / max(got, 1)) + t_drift
-    return {"value": N / t_step, "unit": "particle-steps/s", "cores": ncores, "kind": "port",
-            "sample": "%s: full tree build (%.1f s, 1 thread) + drift, kick on every %d-th top-level work item (%d of %d particles, %.1f s, %d threads), "
-                      "kick time scaled to all particles" % (workload_name(args), t_tree, stride, got, N, dt, ncores)}
+    st = {"x": x.copy(), "y": y.copy(), "z": z.copy(), "v": v.copy(), "rung": np.zeros(N, np.int8), "rung_begin": 0, "stack": []}
+    minrung, max_rung = 0, 0
+    if g is not None:
+        minrung, max_rung = oracle_lib.rung_state_from_forces(O, st, g, t0, ics.eta_default(), h)
+    sp = dict(minrung=minrung, minrung0=0, max_rung=max_rung, a=1.0, tau=t0, t0=t0, theta=args.theta, hsoft=h, bucket=128, eta=ics.eta_default(),
+              GM=1.0 / N, max_dt=1e30, do_phi=1, nocrop=0 if g is not None else 1, drag=0.0, sign=1.0)
+    return st, sp
 
 
-def cpu_baseline(args):
+def cpu_estimates(args, st0, sp0, frac, repeats, seed):
+    """Estimated CPU seconds of one step from (st0, sp0), `repeats` times with independent
+    samples (tests/oracle_lib.estimate_step_hierarchical on all host threads)."""
+    import copy
+
+    from tests import oracle_lib
+
+    O = oracle_lib.load(build=False)
+    out = []
+    for k in range(repeats):
+        st = copy.deepcopy(st0)
+        sec, est = oracle_lib.estimate_step_hierarchical(O, st, dict(sp0), frac, seed=seed + 7919 * k)
+        out.append((sec, est))
+    return out
+
+
+def cpu_summary(args, N, runs, frac, wall_s, forces="the device's"):
+    secs = np.array([r[0] for r in runs])
+    est = runs[-1][1]
+    vals = N / secs
+    return {"value": float(N / secs.mean()), "unit": "particle-steps/s", "cores": int(est["threads"]), "kind": "port",
+            "repeats": len(runs), "spread": {"min": float(vals.min()), "max": float(vals.max()), "rel_std": float(vals.std() / vals.mean()) if len(vals) > 1 else 0.0},
+            "est_s_per_step": float(secs.mean()), "wall_s": wall_s,
+            "sample": "%s: one hierarchical step (the same ladder of rung sorts, tree builds over the active particles, kicks and drifts as the "
+                      "device step; %d kicks, %.2e active kicks) per repeat; tree builds (%d threads), the top of each walk, sorts and drifts run in "
+                      "full; of %d work items below the top, %d were walked (chosen with probability proportional to a cost proxy, %.0f%% of it "
+                      "covered) and the walk of all items estimated from them (Horvitz-Thompson); starting rungs from %s forces by the rung rule"
+                      % (workload_name(args), est["kicks"], est["active"], est["threads"], est["items"], est["sampled_items"], 100 * frac, forces)}
+
+
+def cpu_baseline(args, state, g, t0):
+    import time as _t
+
     try:
-        return cpu_measure(args)
+        t = _t.perf_counter()
+        st0, sp0 = cpu_start_state(args, state, g, t0)
+        runs = cpu_estimates(args, st0, sp0, frac=0.03, repeats=3, seed=12345)
+        return cpu_summary(args, len(state[0]), runs, 0.03, _t.perf_counter() - t)
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": "particle-steps/s", "cores": os.cpu_count(), "kind": "port", "sample": "failed: %s" % e}
 
 
+def cpu_c1_full():
+    """The CPU oracle on the lattice workload (64^3 Zel'dovich k^-2 lattice, 0.25 spacing RMS,
+    theta 0.7, one all-particles step: tree build, kick, drift) in full on all host threads, no
+    sample and no extrapolation."""
+    from cosmictiger_b200 import ics
+    from tests import oracle_lib
+
+    O = oracle_lib.load(build=False)
+    x, y, z, v, r = ics.zeldovich_lattice(64, index=-2.0, rms_spacing=0.25, seed=3)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    t = time.perf_counter()
+    nodes = O.tree_build(x, y, z, v, r, 0.7, h, 128)
+    kp = oracle_lib.KickParams(sign=1.0, min_rung=0, a=1.0, t0=1.0 / 64, theta=0.7, h=h, eta=ics.eta_default(), GM=1.0 / N, max_dt=1e30,
+                               save_force=0, first_call=1, ascending=1, descending=1, top=1, do_phi=1)
+    O.kick(kp, nodes, x, y, z, v, r, save_force=False)
+    O.drift(x, y, z, v, r, 0, 1.0, 1.0 / 64)
+    return {"seconds": time.perf_counter() - t, "particles": N, "cores": os.cpu_count()}
+
+
+def gpu_c1(ct, torch, ctx, lib_stream):
+    """The same lattice step on the device: device time (CUDA events) and end to end (host
+    buffers in and out) for one all-particles step after one warm-up."""
+    from cosmictiger_b200 import ics
+
+    x, y, z, v, r = ics.zeldovich_lattice(64, index=-2.0, rms_spacing=0.25, seed=3)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    box = ctx.box(N)
+
+    def step():
+        box.upload(x, y, z, v, r)
+        box.tree_create(0.7, h, 128)
+        box.kick(ct.KickParams.make(theta=0.7, h=h, GM=1.0 / N, eta=ics.eta_default(), t0=1.0 / 64, first_call=True, save_force=False))
+        box.drift(0, 1.0, 1.0 / 64)
+        return box.download()
+
+    step()
+    ctx.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t = time.perf_counter()
+    e0.record(lib_stream)
+    step()
+    e1.record(lib_stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t
+    box.close()
+    return {"device_ms": e0.elapsed_time(e1), "e2e_ms": wall * 1e3, "particles": N}
+
+
 def run_reference(args):
-    """The reference arm: the CPU implementation of the path on all host cores (the oracle port;
-    the reference's own CPU kick aborts in P2P, src/gravity.cpp:257-258)."""
-    vals = []
-    info = None
+    """The reference arm: the CPU implementation of the path (the oracle port; the reference's
+    own CPU kick aborts in P2P, src/gravity.cpp:257-258) on all host threads, timing the same
+    step as the device arm.  The forces that set the starting rungs come from one full CPU kick
+    (untimed set-up); every warm-up and timed step is then one estimated hierarchical step from
+    that state with an independent sample."""
+    from cosmictiger_b200 import ics
+    from tests import oracle_lib
+
+    t_all = time.perf_counter()
     state = make_ics(args, seed=3)
-    for i in range(args.warmup + args.steps):
-        m = cpu_measure(args, target_s=max(2.0, 20.0 / max(1, args.steps)), state=state)
-        if i >= args.warmup:
-            vals.append(m["value"])
-            info = m
-    v = float(np.mean(vals))
+    x, y, z, v, r = (a.copy() for a in state)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    O = oracle_lib.load(build=False)
+    g, t0 = None, 1.0 / 64
+    t_setup = time.perf_counter()
+    if args.mode == "multistep":
+        nodes = O.tree_build(x, y, z, v, r, args.theta, h, 128)
+        kp = oracle_lib.KickParams(sign=1.0, min_rung=0, a=1.0, t0=1.0, theta=args.theta, h=h, eta=ics.eta_default(), GM=1.0 / N, max_dt=1e30,
+                                   save_force=1, first_call=1, ascending=0, descending=0, top=1, do_phi=1)
+        (gx, gy, gz, _), _, _ = O.kick(kp, nodes, x, y, z, v.copy(), r.copy())
+        g = np.stack([gx, gy, gz], 1)
+        dts = ics.eta_default() * np.sqrt(h / np.maximum(np.linalg.norm(g.astype(np.float64), axis=1), 1e-30))
+        t0 = float(8.0 * np.percentile(dts, 1))
+    t_setup = time.perf_counter() - t_setup
+    st0, sp0 = cpu_start_state(args, (x, y, z, v, r), g, t0)
+    # each step's sample sized so that warm-up and timed steps together stay within a few minutes
+    frac = float(np.clip(0.03 * 12.0 / max(1, args.steps + args.warmup), 0.005, 0.03))
+    cpu_estimates(args, st0, sp0, frac=0.002, repeats=args.warmup, seed=999)
+    t = time.perf_counter()
+    runs = cpu_estimates(args, st0, sp0, frac=frac, repeats=args.steps, seed=4242)
+    wall = time.perf_counter() - t
+    summ = cpu_summary(args, N, runs, frac, wall, forces="a full CPU kick's")
+    v = summ["value"]
     line = {"impl": "reference", "metric": "particle-steps/s at <=1e-3 rms force err; ensemble-batched vs plain; p50/p99 ms", "value": v,
-            "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * (args.n ** 3) / v,
+            "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * N / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
-            "config": {"workload": workload_name(args), "theta": args.theta, "order": 7, "bucket": 128, "parallelism": "host threads"},
-            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": info["cores"], "kind": "port", "sample": info["sample"]},
-            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": workload_name(args), "particles_per_gpu": N, "theta": args.theta, "order": 7, "bucket": 128, "parallelism": "host threads"},
+            "cpu_baseline": {k: summ[k] for k in ("value", "unit", "cores", "kind", "sample", "repeats", "spread")},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "extrapolated": {"what": "ms_per_step is the estimated full CPU step; each timed step walks a sampled %.1f%% (by cost proxy) of the "
+                                     "work items and runs tree builds, walk tops, sorts and drifts in full" % (100 * frac),
+                             "measured_ms_per_step": 1e3 * wall / max(1, args.steps), "setup_full_kick_s": t_setup,
+                             "run_s": time.perf_counter() - t_all}}
     print(json.dumps(line), flush=True)
 
 

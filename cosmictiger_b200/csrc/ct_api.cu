@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "ct_internal.cuh"
@@ -390,8 +391,9 @@ ct_status drift_run(Ctx* c, Box* b, int rung, float a, float dt, double drag, bo
 ct_status sort_by_rung_run(Ctx* c, Box* b, int minrung) {
 	cudaStream_t st = c->stream;
 	if (minrung == 0) {
+		// particles_sort_by_rung(0) only resets the active range (particles.cpp:1035-1036);
+		// saved ranges on the rung stack stay for the caller's pops
 		b->rung_begin = 0;
-		b->rung_stack.clear();
 		b->tree_valid = false;
 		return CT_OK;
 	}
@@ -439,8 +441,11 @@ ct_status sort_by_rung_run(Ctx* c, Box* b, int minrung) {
 ct_status direct_ewald_run(Ctx* c, Box* b, int64_t nsink, const uint32_t* sx, const uint32_t* sy, const uint32_t* sz, double h, double* gx,
 		double* gy, double* gz, double* pot) {
 	cudaStream_t st = c->stream;
+	// the index table is the same for every call: built once, read-only afterwards (calls from
+	// several host threads on different contexts share it)
 	static ct_p7::EwaldTab tab;
-	ct_p7::ewald_build_indices(tab);
+	static std::once_flag tab_once;
+	std::call_once(tab_once, [] { ct_p7::ewald_build_indices(tab); });
 	ct_status s = CT_OK;
 	float* dreal = (float*) scratch(c, 30, sizeof(tab.real) + sizeof(tab.four), &s);
 	uint32_t* dsk = (uint32_t*) scratch(c, 31, sizeof(uint32_t) * 3 * nsink, &s);

@@ -107,10 +107,10 @@ __device__ __forceinline__ bool lc_crossing(const LcArgs& a, const double p0[3],
 	const double x1 = p1[0] + ox, y1 = p1[1] + oy, z1 = p1[2] + oz;
 	const double dist0 = sqrt(x0 * x0 + y0 * y0 + z0 * z0);
 	const double dist1 = sqrt(x1 * x1 + y1 * y1 + z1 * z1);
-	const double tau0_ = a.t0 + dist0;
-	const double tau1_ = a.t1 + dist1;
-	const int i0 = (int) (tau0_ * a.c0);
-	const int i1 = (int) (tau1_ * a.c0);
+	const double cone0 = a.t0 + dist0;  // tau + distance at the drift's two ends
+	const double cone1 = a.t1 + dist1;
+	const int i0 = (int) (cone0 * a.c0);
+	const int i1 = (int) (cone1 * a.c0);
 	if (!(i0 != i1 && (dist1 <= 1.0 || dist0 <= 1.0))) {
 		return false;
 	}
@@ -120,11 +120,11 @@ __device__ __forceinline__ bool lc_crossing(const LcArgs& a, const double p0[3],
 	const float vz = vel[2] * a.ainv;
 	const double ti = double((double) (i0 + 1)) * double(a.tmax);
 	const double dti = ti - a.t0;
-	const double sqrtauimtau0 = dti * dti;
-	const double tau0mtaui = a.t0 - ti;
+	const double dti2 = dti * dti;
+	const double lag = a.t0 - ti;
 	const double A = 1.0 - (vx * vx + vy * vy + vz * vz);
-	const double B = 2.0 * (tau0mtaui - (vx * x0 + vy * y0 + vz * z0));
-	const double C = sqrtauimtau0 - (x0 * x0 + y0 * y0 + z0 * z0);
+	const double B = 2.0 * (lag - (vx * x0 + vy * y0 + vz * z0));
+	const double C = dti2 - (x0 * x0 + y0 * y0 + z0 * z0);
 	const double t = -(B + sqrt(B * B - 4.0 * A * C)) / (2.0 * A);
 	q[0] = x0 + vx * t;
 	q[1] = y0 + vy * t;

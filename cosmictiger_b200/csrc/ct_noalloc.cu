@@ -82,20 +82,22 @@ __global__ void k_na_positions(int64_t begin, int64_t cnt, const int8_t* rung, i
 	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < cnt; i += (int64_t) gridDim.x * blockDim.x) {
 		const int64_t p = begin + i;
 		const bool lt = rung[p] < min_rung;
+		// offsets from begin (below the 2^20 capacity), so that no index wraps however far
+		// into the caller's arrays the range starts
 		if (p < s && !lt) {
-			posL[exL[i]] = (int) p;
+			posL[exL[i]] = (int) i;
 		}
 		if (p >= s && lt) {
-			posR[*totR - 1 - exR[i]] = (int) p;
+			posR[*totR - 1 - exR[i]] = (int) i;
 		}
 	}
 }
 
-__global__ void k_na_swap(const int* posL, const int* posR, const int* nmis, uint32_t* x, uint32_t* y, uint32_t* z, float* vx, float* vy, float* vz,
-		int8_t* rung) {
+__global__ void k_na_swap(int64_t begin, const int* posL, const int* posR, const int* nmis, uint32_t* x, uint32_t* y, uint32_t* z, float* vx,
+		float* vy, float* vz, int8_t* rung) {
 	const int n = *nmis;
 	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-		const int a = posL[k], b = posR[k];
+		const int64_t a = begin + posL[k], b = begin + posR[k];
 		uint32_t t = x[a];
 		x[a] = x[b];
 		x[b] = t;
@@ -184,7 +186,7 @@ extern "C" ct_status ct_sort_by_rung_noalloc(int64_t begin, int64_t n, int min_r
 	}
 	const int grid = (int) ((cnt + 255) / 256 < 4096 ? (cnt + 255) / 256 : 4096);
 	k_na_positions<<<grid, 256, 0, st>>>(begin, cnt, rung, min_rung, counters, exL, exR, counters + 2, posL, posR);
-	k_na_swap<<<grid, 256, 0, st>>>(posL, posR, counters + 1, x, y, z, vx, vy, vz, rung);
+	k_na_swap<<<grid, 256, 0, st>>>(begin, posL, posR, counters + 1, x, y, z, vx, vy, vz, rung);
 	int m = 0;
 	e = cudaGetLastError();
 	if (e == cudaSuccess) e = cudaMemcpyAsync(&m, counters, sizeof(int), cudaMemcpyDeviceToHost, st);

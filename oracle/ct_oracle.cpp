@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -188,10 +189,10 @@ struct Builder {
 	int8_t* r;
 	double theta, h;
 	int bucket;
-	ct_or_node* nodes;
-	int max_nodes;
-	int count;
-	bool overflow;
+	// nodes in depth-first order (parent, left subtree, right subtree); a subtree built on
+	// another thread is spliced in after the left one, so the order does not depend on threads
+	std::vector<ct_or_node> nodes;
+	int fork_depth;  // right children above this depth are built on their own thread
 	bool too_deep;  // a node at depth MAX_DEPTH - 1 still had to split (tree.cpp:285-286)
 };
 
@@ -224,10 +225,8 @@ int partition(Builder& B, int b, int e, double xm, int xdim) {
 template<class Ops>
 BuildRet tree_create(Builder& B, uint64_t key, int pb, int pe, const double* box_b, const double* box_e, int depth) {
 	BuildRet rc;
-	const int index = B.count++;
-	if (index >= B.max_nodes) {
-		B.overflow = true;
-	}
+	const int index = (int) B.nodes.size();
+	B.nodes.emplace_back();
 	const int nparts = pe - pb;
 	float box_r = 0.0f;
 	for (int dim = 0; dim < 3; dim++) {
@@ -244,7 +243,7 @@ BuildRet tree_create(Builder& B, uint64_t key, int pb, int pe, const double* box
 	if (must_split && depth >= 127) {
 		B.too_deep = true;
 	}
-	if (!B.overflow && !B.too_deep && must_split) {
+	if (!B.too_deep && must_split) {
 		isleaf = false;
 		int xdim = 0;
 		double max_span = -1.0;
@@ -263,8 +262,42 @@ BuildRet tree_create(Builder& B, uint64_t key, int pb, int pe, const double* box
 			le[d] = re[d] = box_e[d];
 		}
 		le[xdim] = rb[xdim] = xmid;
-		const BuildRet rcl = tree_create<Ops>(B, key << 1, pb, mid, lb, le, depth + 1);
-		const BuildRet rcr = tree_create<Ops>(B, (key << 1) + 1, mid, pe, rb, re, depth + 1);
+		BuildRet rcl, rcr;
+		if (depth < B.fork_depth && nparts > 65536) {
+			// the reference forks the right child (tree.cpp:349-350); here the fork builds into a
+			// builder of its own, whose nodes follow the left subtree's
+			Builder R;
+			for (int d = 0; d < 3; d++) {
+				R.x[d] = B.x[d];
+			}
+			R.v = B.v;
+			R.r = B.r;
+			R.theta = B.theta;
+			R.h = B.h;
+			R.bucket = B.bucket;
+			R.fork_depth = B.fork_depth;
+			R.too_deep = false;
+			std::thread t([&]() {
+				rcr = tree_create<Ops>(R, (key << 1) + 1, mid, pe, rb, re, depth + 1);
+			});
+			rcl = tree_create<Ops>(B, key << 1, pb, mid, lb, le, depth + 1);
+			t.join();
+			const int off = (int) B.nodes.size();
+			for (ct_or_node n : R.nodes) {
+				if (n.child_left >= 0) {
+					n.child_left += off;
+				}
+				if (n.child_right >= 0) {
+					n.child_right += off;
+				}
+				B.nodes.push_back(n);
+			}
+			rcr.id += off;
+			B.too_deep = B.too_deep || R.too_deep;
+		} else {
+			rcl = tree_create<Ops>(B, key << 1, pb, mid, lb, le, depth + 1);
+			rcr = tree_create<Ops>(B, (key << 1) + 1, mid, pe, rb, re, depth + 1);
+		}
 		const float ml0 = rcl.multi_f[0], mr0 = rcr.multi_f[0];
 		for (int dim = 0; dim < 3; dim++) {
 			if (ml0 != 0.0f && mr0 != 0.0f) {
@@ -430,7 +463,7 @@ BuildRet tree_create(Builder& B, uint64_t key, int pb, int pe, const double* box
 	}
 	rc.radius = radius;
 	rc.id = index;
-	if (index < B.max_nodes) {
+	{
 		ct_or_node& n = B.nodes[index];
 		memset(&n, 0, sizeof(n));
 		n.key = key;
@@ -791,35 +824,26 @@ void walk(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const uint3
 	}
 }
 
-// Collect subtrees for parallel processing: the traversal above a cut (nodes larger than
-// max_parts) runs serially and hands each small subtree, with its lists and expansion, to a
-// work item, the same split the reference makes between its CPU top and GPU kernel
-// (kick.cpp:169-190).
+// Work items: the walk above a cut (nodes holding more than max_parts particles that are not
+// leaves) hands each subtree below it, with its check lists and the expansion of its parent,
+// to a work item -- the split the reference makes between its CPU top and its GPU kernel
+// (kick.cpp:169-190), with the items ordered by their first particle as the reference's
+// kick_workspace orders them (kick_workspace.cpp:308-310).  The top runs level by level, the
+// nodes of one level on all threads.
 template<class Ops>
 struct WorkItem {
 	int self;
-	std::vector<float> L;
+	std::vector<float> L;  // the parent's expansion, about Lpos
 	uint32_t pos[3];
 	std::vector<int> e, d;
 };
 
+// One node above the cut: its expansion from the parent's (L2L) and its Ewald and direct
+// check lists (the same list processing as walk() for a non-leaf node); the two children
+// inherit the result.
 template<class Ops>
-void collect(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const uint32_t* Lpos, std::vector<int> echecks, std::vector<int> dchecks,
-		int max_parts, std::vector<WorkItem<Ops>>& items) {
-	const ct_or_node& self = C.nodes[selfi];
-	if (self.leaf || self.part_end - self.part_begin <= max_parts) {
-		WorkItem<Ops> w;
-		w.self = selfi;
-		w.L.assign(Lparent, Lparent + Ops::NEXP);
-		for (int d = 0; d < 3; d++) {
-			w.pos[d] = Lpos[d];
-		}
-		w.e = std::move(echecks);
-		w.d = std::move(dchecks);
-		items.push_back(std::move(w));
-		return;
-	}
-	// Same list processing as walk() for a non-leaf node, then descend.
+void top_expand(KickCtx& C, KickAcc& acc, const WorkItem<Ops>& w, WorkItem<Ops>& left, WorkItem<Ops>& right) {
+	const ct_or_node& self = C.nodes[w.self];
 	const auto& p = *C.p;
 	const ct_or_node* nodes = C.nodes;
 	const bool do_phi = p.do_phi != 0;
@@ -828,13 +852,13 @@ void collect(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const ui
 	float L[Ops::NEXP];
 	float dx[3];
 	for (int d = 0; d < 3; d++) {
-		dx[d] = fdist(self.pos[d], Lpos[d]);
+		dx[d] = fdist(self.pos[d], w.pos[d]);
 	}
-	Ops::l2l(L, Lparent, dx[0], dx[1], dx[2], do_phi);
+	Ops::l2l(L, w.L.data(), dx[0], dx[1], dx[2], do_phi);
 	acc.flops += FLOP_L2L_CUDA + do_phi * FLOP_L2L_PHI;
 	const float rs = self.radius;
 	std::vector<int> cc, next;
-	for (int c : echecks) {
+	for (int c : w.e) {
 		const ct_or_node& o = nodes[c];
 		if (o.part_end - o.part_begin) {
 			for (int d = 0; d < 3; d++) {
@@ -875,7 +899,7 @@ void collect(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const ui
 	cc.clear();
 	next.clear();
 	std::vector<int> leaf;
-	for (int c : dchecks) {
+	for (int c : w.d) {
 		const ct_or_node& o = nodes[c];
 		if (!(o.part_end - o.part_begin)) {
 			continue;
@@ -918,68 +942,166 @@ void collect(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const ui
 			L[i] += Lacc[i];
 		}
 	}
-	collect<Ops>(C, acc, self.child_left, L, self.pos, e2, d2, max_parts, items);
-	collect<Ops>(C, acc, self.child_right, L, self.pos, e2, d2, max_parts, items);
+	for (WorkItem<Ops>* ch : { &left, &right }) {
+		ch->L.assign(L, L + Ops::NEXP);
+		for (int d = 0; d < 3; d++) {
+			ch->pos[d] = self.pos[d];
+		}
+		ch->e = e2;
+		ch->d = d2;
+	}
+	left.self = self.child_left;
+	right.self = self.child_right;
 }
 
-template<class Ops>
-int kick_impl(const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y, const uint32_t* z, float* v,
-		int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops, int stride = 1,
-		int64_t* sampled = nullptr) {
-	if (nnodes <= 0) {
-		return -1;
+struct PlanBase {
+	virtual ~PlanBase() {
 	}
+	ct_or_kick_params p;
 	KickCtx C;
-	C.p = p;
-	C.nodes = nodes;
-	C.x[0] = x;
-	C.x[1] = y;
-	C.x[2] = z;
-	C.v = v;
-	C.rung = rung;
-	C.gx = gx;
-	C.gy = gy;
-	C.gz = gz;
-	C.pot = pot;
-	const int root = 0;
-	float L0[Ops::NEXP] = { };
-	uint32_t pos0[3] = { 0, 0, 0 };
-	std::vector<int> checks(1, root);
+	int order;
+	KickAcc top;
+	double top_seconds = 0.0;
+	virtual int64_t size() const = 0;
+	virtual void info(int32_t* self, int32_t* nparts, int64_t* dsum, int32_t* ne) const = 0;
+	virtual void run(const int8_t* select, int nthreads, double* seconds, KickAcc& tot) = 0;
+};
+
+template<class Ops>
+struct Plan: PlanBase {
+	std::vector<WorkItem<Ops>> items;
+	int64_t size() const override {
+		return (int64_t) items.size();
+	}
+	void build(int max_parts, int nthreads) {
+		const auto t0 = std::chrono::steady_clock::now();
+		std::vector<WorkItem<Ops>> level(1);
+		level[0].self = 0;
+		level[0].L.assign(Ops::NEXP, 0.f);
+		for (int d = 0; d < 3; d++) {
+			level[0].pos[d] = 0;
+		}
+		level[0].e.assign(1, 0);
+		level[0].d.assign(1, 0);
+		while (!level.empty()) {
+			const int n = (int) level.size();
+			std::vector<WorkItem<Ops>> kids(2 * (size_t) n);
+			std::vector<char> expanded(n, 0);
+			std::vector<KickAcc> accs(n);
+			parallel_for(n, nthreads, [&](int i) {
+				const ct_or_node& nd = C.nodes[level[i].self];
+				if (nd.leaf || nd.part_end - nd.part_begin <= max_parts) {
+					return;
+				}
+				top_expand<Ops>(C, accs[i], level[i], kids[2 * i], kids[2 * i + 1]);
+				expanded[i] = 1;
+			});
+			std::vector<WorkItem<Ops>> nextl;
+			for (int i = 0; i < n; i++) {
+				top.flops += accs[i].flops;
+				if (expanded[i]) {
+					nextl.push_back(std::move(kids[2 * i]));
+					nextl.push_back(std::move(kids[2 * i + 1]));
+				} else {
+					items.push_back(std::move(level[i]));
+				}
+			}
+			level.swap(nextl);
+		}
+		std::stable_sort(items.begin(), items.end(), [&](const WorkItem<Ops>& a, const WorkItem<Ops>& b) {
+			return C.nodes[a.self].part_begin < C.nodes[b.self].part_begin;
+		});
+		top_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+	}
+	void info(int32_t* self, int32_t* nparts, int64_t* dsum, int32_t* ne) const override {
+		for (size_t i = 0; i < items.size(); i++) {
+			const ct_or_node& nd = C.nodes[items[i].self];
+			if (self) {
+				self[i] = items[i].self;
+			}
+			if (nparts) {
+				nparts[i] = nd.part_end - nd.part_begin;
+			}
+			if (dsum) {
+				int64_t s = 0;
+				for (int c : items[i].d) {
+					s += C.nodes[c].part_end - C.nodes[c].part_begin;
+				}
+				dsum[i] = s;
+			}
+			if (ne) {
+				ne[i] = (int32_t) items[i].e.size();
+			}
+		}
+	}
+	void run(const int8_t* select, int nthreads, double* seconds, KickAcc& tot) override {
+		std::vector<int> todo;
+		for (int i = 0; i < (int) items.size(); i++) {
+			if (!select || select[i]) {
+				todo.push_back(i);
+			}
+		}
+		std::vector<KickAcc> accs(todo.size());
+		parallel_for((int) todo.size(), nthreads, [&](int k) {
+			const int i = todo[k];
+			const auto t0 = std::chrono::steady_clock::now();
+			walk<Ops>(C, accs[k], items[i].self, items[i].L.data(), items[i].pos, items[i].e, items[i].d);
+			if (seconds) {
+				seconds[i] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+			}
+		});
+		tot = top;
+		for (auto& a : accs) {
+			tot.max_rung = std::max(tot.max_rung, a.max_rung);
+			tot.pot += a.pot;
+			tot.kin += a.kin;
+			tot.dkin += a.dkin;
+			tot.xmom += a.xmom;
+			tot.ymom += a.ymom;
+			tot.zmom += a.zmom;
+			tot.nmom += a.nmom;
+			tot.flops += a.flops;
+		}
+	}
+};
+
+PlanBase* make_plan(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y,
+		const uint32_t* z, int max_parts, int nthreads) {
+	if (nnodes <= 0) {
+		return nullptr;
+	}
+	PlanBase* P;
+	if (order == 5) {
+		P = new Plan<Ops5>();
+	} else {
+		P = new Plan<Ops7>();
+	}
+	P->order = order;
+	P->p = *p;
+	P->C.p = &P->p;
+	P->C.nodes = nodes;
+	P->C.x[0] = x;
+	P->C.x[1] = y;
+	P->C.x[2] = z;
+	P->C.v = nullptr;
+	P->C.rung = nullptr;
+	P->C.gx = P->C.gy = P->C.gz = P->C.pot = nullptr;
 	if (nthreads <= 0) {
 		nthreads = std::max(1u, std::thread::hardware_concurrency());
 	}
-	const int ntot = nodes[root].part_end - nodes[root].part_begin;
-	const int max_parts = std::max(ntot / std::max(1, 16 * nthreads), 1);
-	KickAcc top;
-	std::vector<WorkItem<Ops>> items;
-	collect<Ops>(C, top, root, L0, pos0, checks, checks, max_parts, items);
-	// a sampled run processes every stride-th work item (bounded CPU baseline)
-	std::vector<int> todo;
-	int64_t nsamp = 0;
-	for (int i = 0; i < (int) items.size(); i += std::max(stride, 1)) {
-		todo.push_back(i);
-		nsamp += nodes[items[i].self].part_end - nodes[items[i].self].part_begin;
+	if (max_parts <= 0) {
+		const int ntot = nodes[0].part_end - nodes[0].part_begin;
+		max_parts = std::max(ntot / std::max(1, 16 * nthreads), 1);
 	}
-	if (sampled) {
-		*sampled = nsamp;
+	if (order == 5) {
+		static_cast<Plan<Ops5>*>(P)->build(max_parts, nthreads);
+	} else {
+		static_cast<Plan<Ops7>*>(P)->build(max_parts, nthreads);
 	}
-	std::vector<KickAcc> accs(items.size());
-	parallel_for((int) todo.size(), nthreads, [&](int k) {
-		const int i = todo[k];
-		walk<Ops>(C, accs[i], items[i].self, items[i].L.data(), items[i].pos, items[i].e, items[i].d);
-	});
-	KickAcc tot = top;
-	for (auto& a : accs) {
-		tot.max_rung = std::max(tot.max_rung, a.max_rung);
-		tot.pot += a.pot;
-		tot.kin += a.kin;
-		tot.dkin += a.dkin;
-		tot.xmom += a.xmom;
-		tot.ymom += a.ymom;
-		tot.zmom += a.zmom;
-		tot.nmom += a.nmom;
-		tot.flops += a.flops;
-	}
+	return P;
+}
+
+void store_return(const KickAcc& tot, ct_or_kick_return* rc, double* flops) {
 	if (rc) {
 		rc->max_rung = tot.max_rung;
 		rc->pot = tot.pot;
@@ -993,6 +1115,22 @@ int kick_impl(const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, c
 	if (flops) {
 		*flops = tot.flops;
 	}
+}
+
+int plan_run(PlanBase* P, float* v, int8_t* rung, float* gx, float* gy, float* gz, float* pot, const int8_t* select, int nthreads,
+		double* seconds, ct_or_kick_return* rc, double* flops) {
+	if (P->p.save_force && (!gx || !gy || !gz || !pot)) {
+		return -2;
+	}
+	P->C.v = v;
+	P->C.rung = rung;
+	P->C.gx = gx;
+	P->C.gy = gy;
+	P->C.gz = gz;
+	P->C.pot = pot;
+	KickAcc tot;
+	P->run(select, nthreads, seconds, tot);
+	store_return(tot, rc, flops);
 	return 0;
 }
 
@@ -1094,7 +1232,7 @@ void ct_or_ewald_tables(int order, float* real_idx, float* four_idx, float* four
 }
 
 int ct_or_tree_build(int order, int n, int begin, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, double theta, double hsoft,
-		int bucket, ct_or_node* nodes, int max_nodes) {
+		int bucket, ct_or_node* nodes, int max_nodes, int nthreads) {
 	Builder B;
 	B.x[0] = x;
 	B.x[1] = y;
@@ -1104,11 +1242,16 @@ int ct_or_tree_build(int order, int n, int begin, uint32_t* x, uint32_t* y, uint
 	B.theta = theta;
 	B.h = hsoft;
 	B.bucket = bucket;
-	B.nodes = nodes;
-	B.max_nodes = max_nodes;
-	B.count = 0;
-	B.overflow = false;
 	B.too_deep = false;
+	if (nthreads <= 0) {
+		nthreads = std::max(1u, std::thread::hardware_concurrency());
+	}
+	// about two subtrees per thread
+	B.fork_depth = 0;
+	while ((1 << B.fork_depth) < 2 * nthreads && nthreads > 1) {
+		B.fork_depth++;
+	}
+	B.nodes.reserve(std::max(64, 2 * (n - begin) / std::max(bucket / 2, 1)));
 	const double bb[3] = { 0, 0, 0 }, be[3] = { 1, 1, 1 };
 	if (order == 5) {
 		tree_create<Ops5>(B, 1, begin, n, bb, be, 0);
@@ -1118,10 +1261,11 @@ int ct_or_tree_build(int order, int n, int begin, uint32_t* x, uint32_t* y, uint
 	if (B.too_deep) {
 		return -2;
 	}
-	if (B.overflow) {
+	if ((int64_t) B.nodes.size() > max_nodes) {
 		return -1;
 	}
-	return B.count;
+	memcpy(nodes, B.nodes.data(), sizeof(ct_or_node) * B.nodes.size());
+	return (int) B.nodes.size();
 }
 
 int ct_or_kick(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y, const uint32_t* z,
@@ -1129,22 +1273,40 @@ int ct_or_kick(int order, const ct_or_kick_params* p, int nnodes, const ct_or_no
 	if (p->save_force && (!gx || !gy || !gz || !pot)) {
 		return -2;
 	}
-	if (order == 5) {
-		return kick_impl<Ops5>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops);
+	PlanBase* P = make_plan(order, p, nnodes, nodes, x, y, z, 0, nthreads);
+	if (!P) {
+		return -1;
 	}
-	return kick_impl<Ops7>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops);
+	const int err = plan_run(P, vxyz, rung, gx, gy, gz, pot, nullptr, nthreads, nullptr, rc, flops);
+	delete P;
+	return err;
 }
 
-int ct_or_kick_sampled(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y,
-		const uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops,
-		int stride, int64_t* sampled) {
-	if (p->save_force && (!gx || !gy || !gz || !pot)) {
-		return -2;
+void* ct_or_kick_plan_create(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y,
+		const uint32_t* z, int max_parts, int nthreads, int64_t* nitems, double* top_seconds) {
+	PlanBase* P = make_plan(order, p, nnodes, nodes, x, y, z, max_parts, nthreads);
+	if (P) {
+		if (nitems) {
+			*nitems = P->size();
+		}
+		if (top_seconds) {
+			*top_seconds = P->top_seconds;
+		}
 	}
-	if (order == 5) {
-		return kick_impl<Ops5>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops, stride, sampled);
-	}
-	return kick_impl<Ops7>(p, nnodes, nodes, x, y, z, vxyz, rung, gx, gy, gz, pot, rc, nthreads, flops, stride, sampled);
+	return P;
+}
+
+void ct_or_kick_plan_items(const void* plan, int32_t* self, int32_t* nparts, int64_t* near_parts, int32_t* ewald_checks) {
+	static_cast<const PlanBase*>(plan)->info(self, nparts, near_parts, ewald_checks);
+}
+
+int ct_or_kick_plan_run(void* plan, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, const int8_t* select, int nthreads,
+		double* item_seconds, ct_or_kick_return* rc, double* flops) {
+	return plan_run(static_cast<PlanBase*>(plan), vxyz, rung, gx, gy, gz, pot, select, nthreads, item_seconds, rc, flops);
+}
+
+void ct_or_kick_plan_destroy(void* plan) {
+	delete static_cast<PlanBase*>(plan);
 }
 
 void ct_or_drift(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt, double drag) {

@@ -72,20 +72,34 @@ typedef struct {
 /* Build the tree over particles [begin, n) in place (reorders x,y,z,v,rung exactly as the
  * reference's partition does).  Returns the node count, -1 if max_nodes is too small, or -2
  * if a node at depth 127 still had to split (more than a bucket of coincident particles), where
- * the reference throws "Maximum depth exceeded" (tree.cpp:285-286, MAX_DEPTH 128). */
+ * the reference throws "Maximum depth exceeded" (tree.cpp:285-286, MAX_DEPTH 128).
+ * Subtrees near the root are built on up to nthreads threads (<= 0: all cores), as the
+ * reference forks its right children (tree.cpp:349-350); the result does not depend on it. */
 int ct_or_tree_build(int order, int n, int begin, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, int8_t* rung, double theta, double hsoft,
-		int bucket, ct_or_node* nodes, int max_nodes);
+		int bucket, ct_or_node* nodes, int max_nodes, int nthreads);
 
 /* Kick over a tree built by ct_or_tree_build.  g/pot may be null unless save_force.
  * nthreads <= 0 uses every available core. */
 int ct_or_kick(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y, const uint32_t* z,
 		float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops);
 
-/* Same kick on every stride-th top-level work item only (a bounded sample for CPU timing);
- * *sampled receives the number of particles kicked. */
-int ct_or_kick_sampled(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y,
-		const uint32_t* z, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, ct_or_kick_return* rc, int nthreads, double* flops,
-		int stride, int64_t* sampled);
+/* The kick as work items.  ct_or_kick_plan_create runs the top of the walk (every node holding
+ * more than max_parts particles that is not a leaf; max_parts <= 0: total / (16 nthreads)) on
+ * nthreads threads, level by level, and keeps the subtrees below it as work items with their
+ * check lists and parent expansions, ordered by first particle (the reference's CPU top and its
+ * GPU work items, kick.cpp:150-507, kick_workspace.cpp:308-310).  The plan keeps pointers to
+ * `nodes` and the positions, which must outlive it.
+ * ct_or_kick_plan_items: per item its subtree root, particle count, the particles in its
+ * direct check list and the length of its Ewald check list.
+ * ct_or_kick_plan_run: walks the items with select[i] != 0 (NULL: all) -- only their particles
+ * are kicked -- and stores each walked item's wall time in item_seconds (may be NULL); the
+ * return sums the walked items and the top's flops.  A plan may run several times. */
+void* ct_or_kick_plan_create(int order, const ct_or_kick_params* p, int nnodes, const ct_or_node* nodes, const uint32_t* x, const uint32_t* y,
+		const uint32_t* z, int max_parts, int nthreads, int64_t* nitems, double* top_seconds);
+void ct_or_kick_plan_items(const void* plan, int32_t* self, int32_t* nparts, int64_t* near_parts, int32_t* ewald_checks);
+int ct_or_kick_plan_run(void* plan, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, const int8_t* select, int nthreads,
+		double* item_seconds, ct_or_kick_return* rc, double* flops);
+void ct_or_kick_plan_destroy(void* plan);
 
 /* Drift of one rung (src/drift.cu:36-154, lightcone excluded). */
 void ct_or_drift(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt, double drag);

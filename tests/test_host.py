@@ -214,3 +214,42 @@ def test_header_compiles_and_links_from_c_and_cpp(tmp_path, compiler, std):
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert run.returncode == 0, run.stdout + run.stderr
     assert run.stdout.startswith(("context order 7", "status -")), run.stdout
+
+
+def test_noalloc_rung_partition_rejects_bad_arguments_before_device_work():
+    """ct_sort_by_rung_noalloc checks its arguments before it touches a device: a negative
+    begin, n below begin, min_rung outside 0-15, NULL arrays for a non-empty range and a null
+    result pointer give CT_ERR_ARG; a range above the fixed capacity gives CT_ERR_CAPACITY;
+    min_rung 0 and an empty range succeed without device work.  None of these calls needs a
+    GPU, so they run here (in a child process, so that a crash fails the test)."""
+    import cosmictiger_b200 as ct
+
+    ct.library()
+    prog = r'''
+import ctypes, sys
+sys.path.insert(0, %r)
+import cosmictiger_b200 as ct
+f = ct.library().ct_sort_by_rung_noalloc
+vp = ctypes.c_void_p
+f.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int, vp, vp, vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64), vp]
+f.restype = ctypes.c_int
+buf = (ctypes.c_uint8 * 64)()
+a = ctypes.cast(buf, vp)
+def call(begin, n, mr, arrays=True, out=True):
+    rb = ctypes.c_int64(-7)
+    args = [a] * 7 if arrays else [None] * 7
+    rc = f(begin, n, mr, *args, ctypes.byref(rb) if out else None, None)
+    return rc, rb.value
+cap = 1 << 20
+print(call(-1, 10, 1)[0], call(5, 4, 1)[0], call(0, 10, 16)[0], call(0, 10, -1)[0], call(0, 10, 1, arrays=False)[0], call(0, 10, 1, out=False)[0])
+print(call(3, 3 + cap + 1, 1)[0], call(0, cap + 1, 1, arrays=False)[0])
+print(*call(4, 100, 0), *call(9, 9, 2))
+''' % ROOT
+    out = subprocess.run([sys.executable, "-c", prog], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = out.stdout.split("\n")
+    arg = [int(t) for t in lines[0].split()]
+    assert arg == [-1] * 6, arg  # CT_ERR_ARG
+    assert [int(t) for t in lines[1].split()] == [-4, -4]  # CT_ERR_CAPACITY
+    # min_rung 0 resets the active range to 0; an empty range leaves it at begin
+    assert [int(t) for t in lines[2].split()] == [0, 0, 0, 9]

@@ -79,3 +79,52 @@ def test_noalloc_rejects_oversize():
     rc = f(0, n, 1, None, None, None, None, None, None, None, ctypes.byref(rb), None)
     assert rc == -4  # CT_ERR_CAPACITY, before any device work
     assert rb.value == -1
+
+
+def test_noalloc_full_capacity_from_an_offset():
+    """The largest call the fixed scratch array allows (exactly CT_NOALLOC_MAX_PARTICLES
+    particles) on a range that starts past the beginning of the caller's arrays, against
+    ct_sort_by_rung on the same data: the active range of a previous partition (rung 0 moved
+    to the front) is partitioned again at min_rung 3."""
+    import torch
+
+    import cosmictiger_b200 as ct
+
+    lib = ct.library()
+    f = _noalloc(lib)
+    cap = 1 << 20
+    n0 = 5003  # particles on rung 0, in front of the active range after the first partition
+    N = n0 + cap
+    rng = np.random.default_rng(77)
+    x, y, z = (rng.integers(0, 2 ** 32, N, dtype=np.uint64).astype(np.uint32) for _ in range(3))
+    v = rng.standard_normal((N, 3)).astype(np.float32)
+    r = rng.integers(1, 6, N).astype(np.int8)
+    r[rng.choice(N, n0, replace=False)] = 0
+
+    ctx = ct.Context(order=7)
+    box = ctx.box(N)
+    box.upload(x, y, z, v, r)
+    b1 = box.sort_by_rung(1)
+    assert b1 == n0
+    mid = box.download()
+    b3 = box.sort_by_rung(3)
+    ref = box.download()
+    box.close()
+    ctx.close()
+
+    dev = torch.device("cuda", 0)
+    tx, ty, tz = (torch.from_numpy(mid[c].view(np.int32).copy()).to(dev) for c in "xyz")
+    tv = [torch.from_numpy(np.ascontiguousarray(mid["v"][:, d])).to(dev) for d in range(3)]
+    tr = torch.from_numpy(mid["rung"].copy()).to(dev)
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    stream = torch.cuda.current_stream(dev)
+    rb = ctypes.c_int64(-1)
+    rc = f(b1, N, 3, ptr(tx), ptr(ty), ptr(tz), ptr(tv[0]), ptr(tv[1]), ptr(tv[2]), ptr(tr), ctypes.byref(rb), ctypes.c_void_p(stream.cuda_stream))
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert rb.value == b3
+    for c, t in zip("xyz", (tx, ty, tz)):
+        assert np.array_equal(t.cpu().numpy().view(np.uint32), ref[c]), c
+    for d in range(3):
+        assert np.array_equal(tv[d].cpu().numpy(), ref["v"][:, d])
+    assert np.array_equal(tr.cpu().numpy(), ref["rung"])
