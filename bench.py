@@ -446,7 +446,12 @@ def main():
     if args.accuracy_sinks:
         # every rank checks its own box (rank 0 reports), so that no rank waits at the barrier
         # below for another's check
-        acc = accuracy(box, args.accuracy_sinks, h, N)
+        def steps_fn(th):
+            box.upload(x, y, z, v, r)
+            box.sort_by_rung(0)
+            return timed_steps(torch, ctx, box, th, h, N, 2, lib_stream)
+
+        acc = accuracy(box, args.accuracy_sinks, h, N, theta, steps_fn=steps_fn if world == 1 else None)
     cpu = None
     c1 = None
     if not args.no_cpu and rank == 0 and world == 1:
@@ -512,30 +517,76 @@ def read_traffic():
     return None
 
 
-def accuracy(box, nsink, h, N):
-    """Force error of the last kick vs the FP64 direct Ewald sum on nsink seeded sinks."""
-    import cosmictiger_b200 as ct
-
-    st = box.download(forces=False)
-    rng = np.random.default_rng(4321 + 42)
-    sel = np.sort(rng.choice(N, size=min(nsink, N), replace=False))
-    # recompute forces at the current positions (a kick with save_force)
-    box.tree_create(box.tree_params.theta, h, 128)
-    kp = ct.KickParams.make(theta=box.tree_params.theta, h=h, GM=1.0 / N, eta=0.25 / np.sqrt(693 / 256.0), save_force=True, descending=False,
-                            ascending=False)
-    box.kick(kp)
-    out = box.download(forces=True)
-    dg = box.direct_ewald(out["x"][sel], out["y"][sel], out["z"][sel], h)
-    gt = np.stack([out["gx"][sel], out["gy"][sel], out["gz"][sel]], 1).astype(np.float64)
-    gd = np.stack(dg[:3], 1) / N
+def _errors(gt, gd):
     err = np.linalg.norm(gt - gd, axis=1) / np.linalg.norm(gd, axis=1)
     mag = np.abs(np.linalg.norm(gt, axis=1) - np.linalg.norm(gd, axis=1)) / np.linalg.norm(gd, axis=1)
-    del st
-    return {"sinks": int(len(sel)), "rms": float(np.sqrt(np.sum((gt - gd) ** 2) / np.sum(gd ** 2))),
-            "rms_per_particle": float(np.sqrt(np.mean(err ** 2))), "p99_per_particle": float(np.percentile(err, 99)),
-            "mag_p50": float(np.percentile(mag, 50)), "mag_p99": float(np.percentile(mag, 99)),
-            "definition": "vs FP64 direct Ewald on seeded sinks: rms = sqrt(sum|dg|^2 / sum|g|^2); per_particle = |dg|/|g| per sink "
-                          "(rms and 99th percentile); mag = ||g|-|g_ref||/|g_ref| (the reference's force test, analytic.cpp:78-89)"}
+    return {"rms": float(np.sqrt(np.sum((gt - gd) ** 2) / np.sum(gd ** 2))), "rms_per_particle": float(np.sqrt(np.mean(err ** 2))),
+            "p99_per_particle": float(np.percentile(err, 99)), "mag_p50": float(np.percentile(mag, 50)), "mag_p99": float(np.percentile(mag, 99))}
+
+
+def _pos_key(x, y, z):
+    return (x.astype(np.uint64) << np.uint64(32)) | y.astype(np.uint64), z
+
+
+def accuracy(box, nsink, h, N, theta, gate_thetas=(0.5, 0.45, 0.4, 0.35), steps_fn=None):
+    """Force error of the kick vs the FP64 direct Ewald sum on nsink seeded sinks at the run's
+    theta, and the force-error gate: the same sinks (matched by position; the positions do not
+    move) at smaller theta, each with the particle-steps/s of the all-particles step
+    (steps_fn(theta) -> ms), until one passes 1e-3 per-particle RMS."""
+    import cosmictiger_b200 as ct
+
+    rng = np.random.default_rng(4321 + 42)
+    base = box.download()  # every kick below starts from these positions (timing steps move them)
+
+    def kick_at(th):
+        box.upload(base["x"], base["y"], base["z"], base["v"], base["rung"])
+        box.sort_by_rung(0)
+        box.tree_create(th, h, 128)
+        box.kick(ct.KickParams.make(theta=th, h=h, GM=1.0 / N, eta=0.25 / np.sqrt(693 / 256.0), save_force=True, descending=False, ascending=False))
+        return box.download(forces=True)
+
+    out = kick_at(theta)
+    sel = np.sort(rng.choice(N, size=min(nsink, N), replace=False))
+    sx, sy, sz = out["x"][sel], out["y"][sel], out["z"][sel]
+    dg = box.direct_ewald(sx, sy, sz, h)
+    gd = np.stack(dg[:3], 1) / N
+    gt = np.stack([out["gx"][sel], out["gy"][sel], out["gz"][sel]], 1).astype(np.float64)
+    res = {"sinks": int(len(sel)), **_errors(gt, gd),
+           "definition": "vs FP64 direct Ewald on seeded sinks: rms = sqrt(sum|dg|^2 / sum|g|^2) (the global norm, dominated by the largest "
+                         "forces); per_particle = |dg|/|g| per sink, its rms and 99th percentile (every sink weighted alike, as the "
+                         "reference's force test reads its sinks one by one, analytic.cpp:78-89); mag = ||g|-|g_ref||/|g_ref| (that test's "
+                         "own measure)"}
+    del out
+    # the gate: the sinks' rows in each new tree order, by position
+    k0, z0 = _pos_key(sx, sy, sz)
+    order0 = np.lexsort((z0, k0))
+    rows = [{"theta": theta, **{k: res[k] for k in ("rms", "rms_per_particle", "p99_per_particle")}}]
+    if steps_fn:
+        rows[0]["ms_all_particles_step"] = steps_fn(theta)
+        rows[0]["particle_steps_s"] = N / (rows[0]["ms_all_particles_step"] / 1e3)
+    for th in gate_thetas:
+        if rows[-1]["rms_per_particle"] <= 1e-3:
+            break
+        o = kick_at(th)
+        k, zz = _pos_key(o["x"], o["y"], o["z"])
+        ordr = np.lexsort((zz, k))
+        pos = np.searchsorted(k[ordr], k0[order0])
+        idx = ordr[pos]
+        assert np.array_equal(k[idx], k0[order0]) and np.array_equal(zz[idx], z0[order0])
+        g2 = np.empty_like(gt)
+        g2[order0] = np.stack([o["gx"][idx], o["gy"][idx], o["gz"][idx]], 1)
+        del o
+        e = _errors(g2, gd)
+        row = {"theta": th, **{q: e[q] for q in ("rms", "rms_per_particle", "p99_per_particle")}}
+        if steps_fn:
+            row["ms_all_particles_step"] = steps_fn(th)
+            row["particle_steps_s"] = N / (row["ms_all_particles_step"] / 1e3)
+        rows.append(row)
+    passing = [r for r in rows if r["rms_per_particle"] <= 1e-3]
+    res["gate"] = {"order": 7, "rows": rows, "threshold": 1e-3,
+                   "passes_global_rms": rows[0]["theta"] if rows[0]["rms"] <= 1e-3 else None,
+                   "passes_per_particle_rms": passing[0]["theta"] if passing else None}
+    return res
 
 
 def cpu_start_state(args, state, g, t0):
