@@ -51,6 +51,7 @@ def parse():
                     help="multistep: hierarchical rung ladder (kick_step_hierarchical); single: all particles every step")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own CUDA kick on the same box")
     ap.add_argument("--accuracy-sinks", type=int, default=10000, help="FP64 direct-Ewald check on this many seeded sinks (0: skip)")
     ap.add_argument("--ensemble-boxes", type=int, default=64, help="boxes of the batched-vs-plain ensemble comparison (0: skip)")
     ap.add_argument("--ensemble-nmin", type=int, default=16)
@@ -462,6 +463,12 @@ def main():
             c1["e2e_speedup"] = c1["cpu_full"]["seconds"] * 1e3 / c1["gpu"]["e2e_ms"]
         except Exception as e:  # reported, never required
             c1 = {"failed": str(e)}
+    ref_gpu = None
+    if not args.no_ref_gpu and rank == 0 and world == 1:
+        try:
+            ref_gpu = reference_gpu_compare(ct, torch, ctx, lib_stream, args)
+        except Exception as e:  # reported, never required
+            ref_gpu = {"failed": str(e)}
     if pg:
         pg.barrier()
     if rank == 0:
@@ -496,6 +503,8 @@ def main():
             line["multistep"] = multistep
         if c1:
             line["c1_unsampled"] = c1
+        if ref_gpu:
+            line["ref_gpu"] = ref_gpu
         print(json.dumps(line), flush=True)
     box.close()
     ctx.close()
@@ -703,6 +712,71 @@ def gpu_c1(ct, torch, ctx, lib_stream):
     wall = time.perf_counter() - t
     box.close()
     return {"device_ms": e0.elapsed_time(e1), "e2e_ms": wall * 1e3, "particles": N}
+
+
+def reference_gpu_compare(ct, torch, ctx, lib_stream, args):
+    """The reference's own CUDA kick (src/kick.cu cuda_kick_kernel, compiled from its sources
+    for sm_100a, oracle/_ref/libctref_gpu.so) in its production form on the benchmark box: the
+    CPU top of the walk (the oracle's restatement) hands subtrees of at most max_parts particles
+    (kick.cpp:173-177) to cuda_execute_kicks as work items.  The same tree (the oracle's,
+    bit-identical to this project's) and particles; every particle kicked once (first call,
+    single rung).  Milliseconds of the second of two calls each (CUDA events; the reference's
+    around cuda_execute_kicks, this project's around ct_kick), and the force difference."""
+    from cosmictiger_b200 import ics
+    from tests import oracle_lib
+    from tests import reference_gpu_lib as rg
+
+    if not rg.available():
+        return {"unavailable": "oracle/_ref/libctref_gpu.so not built (it is compiled from the reference's sources where they are present)"}
+    O = oracle_lib.load(build=False)
+    ref = rg.ReferenceGPU(heap_bytes=16 << 30)
+    x, y, z, v, r = make_ics(args, seed=3)
+    N = len(x)
+    h = ics.softening(N, 0.02)
+    eta = ics.eta_default()
+    theta = args.theta
+    t0 = 1.0 / 64
+    t = time.perf_counter()
+    nodes = O.tree_build(x, y, z, v, r, theta, h, 128)
+    t_tree = time.perf_counter() - t
+    okp = oracle_lib.KickParams(sign=1.0, min_rung=0, a=1.0, t0=t0, theta=theta, h=h, eta=eta, GM=1.0 / N, max_dt=1e30, save_force=1, first_call=1,
+                                ascending=1, descending=1, top=1, do_phi=1)
+    mp = ref.max_parts(N)
+    plan = O.plan(okp, nodes, x, y, z, max_parts=mp)
+    items = plan.export()
+    top_s = plan.top_seconds
+    plan.close()
+    rp = rg.RefKickParams(sign=1.0, min_rung=0, a=1.0, t0=t0, theta=theta, h=h, eta=eta, GM=1.0 / N, max_dt=1e30, save_force=1, first_call=1,
+                          ascending=1, descending=1, top=1, do_phi=1)
+    state = {"x": x, "y": y, "z": z, "v": v, "rung": r}
+    ro = ref.kick_items(state, nodes, rp, items, repeats=2)
+    box = ctx.box(N)
+    box.upload(x, y, z, v, r)
+    box.tree_create(theta, h, 128)
+    kp = ct.KickParams.make(theta=theta, h=h, GM=1.0 / N, eta=eta, t0=t0, first_call=True, save_force=True)
+    ms = []
+    for i in range(2):
+        ctx.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        box.kick(kp)
+        e1.record(lib_stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    out = box.download(forces=True)
+    box.close()
+    g1 = np.stack([out["gx"], out["gy"], out["gz"]], 1).astype(np.float64)
+    g0 = np.stack([ro["gx"], ro["gy"], ro["gz"]], 1).astype(np.float64)
+    ferr = float(np.sqrt(np.sum((g1 - g0) ** 2) / np.sum(g0 ** 2)))
+    perr = float(np.sqrt(np.sum((out["pot"].astype(np.float64) - ro["pot"]) ** 2) / np.sum(ro["pot"].astype(np.float64) ** 2)))
+    return {"what": "all-particles kick of the benchmark box (same tree and particles): the reference's cuda_kick_kernel on production work items "
+                    "vs this project's kick (walk, interaction kernels, leaf kick)",
+            "workload": workload_name(args).replace("4-rung hierarchical steps", "one all-particles kick"), "particles": N,
+            "reference_ms": ro["ms"][-1], "this_ms": ms[-1], "speedup": ro["ms"][-1] / ms[-1], "reference_ms_calls": ro["ms"], "this_ms_calls": ms,
+            "work_items": int(len(items["self"])), "max_parts": mp, "reference_blocks": ref.kick_block_count(),
+            "cpu_top_s": top_s, "cpu_tree_s": t_tree, "force_rel_rms": ferr, "potential_rel_rms": perr}
 
 
 def run_reference(args):

@@ -965,6 +965,8 @@ struct PlanBase {
 	virtual int64_t size() const = 0;
 	virtual void info(int32_t* self, int32_t* nparts, int64_t* dsum, int32_t* ne) const = 0;
 	virtual void run(const int8_t* select, int nthreads, double* seconds, KickAcc& tot) = 0;
+	virtual void list_sizes(int64_t* nd, int64_t* ne) const = 0;
+	virtual void export_items(int32_t* self, float* L, int nexp, uint32_t* pos, int64_t* doff, int32_t* dlist, int64_t* eoff, int32_t* elist) const = 0;
 };
 
 template<class Ops>
@@ -1033,6 +1035,36 @@ struct Plan: PlanBase {
 				ne[i] = (int32_t) items[i].e.size();
 			}
 		}
+	}
+	void list_sizes(int64_t* nd, int64_t* ne) const override {
+		*nd = *ne = 0;
+		for (const auto& w : items) {
+			*nd += (int64_t) w.d.size();
+			*ne += (int64_t) w.e.size();
+		}
+	}
+	void export_items(int32_t* self, float* L, int nexp, uint32_t* pos, int64_t* doff, int32_t* dlist, int64_t* eoff, int32_t* elist) const override {
+		int64_t d = 0, e = 0;
+		for (size_t i = 0; i < items.size(); i++) {
+			const auto& w = items[i];
+			self[i] = w.self;
+			for (int k = 0; k < nexp; k++) {
+				L[i * nexp + k] = k < Ops::NEXP ? w.L[k] : 0.f;
+			}
+			for (int k = 0; k < 3; k++) {
+				pos[3 * i + k] = w.pos[k];
+			}
+			doff[i] = d;
+			eoff[i] = e;
+			for (int c : w.d) {
+				dlist[d++] = c;
+			}
+			for (int c : w.e) {
+				elist[e++] = c;
+			}
+		}
+		doff[items.size()] = d;
+		eoff[items.size()] = e;
 	}
 	void run(const int8_t* select, int nthreads, double* seconds, KickAcc& tot) override {
 		std::vector<int> todo;
@@ -1303,6 +1335,15 @@ void ct_or_kick_plan_items(const void* plan, int32_t* self, int32_t* nparts, int
 int ct_or_kick_plan_run(void* plan, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, const int8_t* select, int nthreads,
 		double* item_seconds, ct_or_kick_return* rc, double* flops) {
 	return plan_run(static_cast<PlanBase*>(plan), vxyz, rung, gx, gy, gz, pot, select, nthreads, item_seconds, rc, flops);
+}
+
+void ct_or_kick_plan_list_sizes(const void* plan, int64_t* ndirect, int64_t* newald) {
+	static_cast<const PlanBase*>(plan)->list_sizes(ndirect, newald);
+}
+
+void ct_or_kick_plan_export(const void* plan, int32_t* self, float* L, int nexp, uint32_t* pos, int64_t* doff, int32_t* dlist, int64_t* eoff,
+		int32_t* elist) {
+	static_cast<const PlanBase*>(plan)->export_items(self, L, nexp, pos, doff, dlist, eoff, elist);
 }
 
 void ct_or_kick_plan_destroy(void* plan) {

@@ -100,6 +100,12 @@ void ct_or_kick_plan_items(const void* plan, int32_t* self, int32_t* nparts, int
 int ct_or_kick_plan_run(void* plan, float* vxyz, int8_t* rung, float* gx, float* gy, float* gz, float* pot, const int8_t* select, int nthreads,
 		double* item_seconds, ct_or_kick_return* rc, double* flops);
 void ct_or_kick_plan_destroy(void* plan);
+/* The work items in the form the reference's cuda_execute_kicks takes them (kick_workitem,
+ * kick.hpp:188-194): subtree root, parent expansion (nexp floats, zero padded), its centre,
+ * and the direct and Ewald check lists (CSR: offsets of nitems + 1 entries). */
+void ct_or_kick_plan_list_sizes(const void* plan, int64_t* ndirect, int64_t* newald);
+void ct_or_kick_plan_export(const void* plan, int32_t* self, float* L, int nexp, uint32_t* pos, int64_t* doff, int32_t* dlist, int64_t* eoff,
+		int32_t* elist);
 
 /* Drift of one rung (src/drift.cu:36-154, lightcone excluded). */
 void ct_or_drift(int n, uint32_t* x, uint32_t* y, uint32_t* z, float* vxyz, const int8_t* rung, int which_rung, float a, float dt, double drag);

@@ -195,6 +195,49 @@ void free_particles() {
 	g_n = 0;
 }
 
+// The caller's tree (this project's exported node layout: ct_node, root at index 0) as the
+// reference's tree_node array with its multi_pos records, in managed memory.
+int lay_out_tree(int64_t nnodes, const ct_node* nodes, tree_node** tn_out, multi_pos** mp_out) {
+	tree_node* tn = managed<tree_node>(nnodes);
+	multi_pos* mp = managed<multi_pos>(nnodes);
+	if (!tn || !mp) {
+		cudaFree(tn);
+		cudaFree(mp);
+		return -1;
+	}
+	for (int64_t i = 0; i < nnodes; i++) {
+		const ct_node& s = nodes[i];
+		tree_node& t = tn[i];
+		memset((void*) &t, 0, sizeof(t));
+		for (int d = 0; d < NDIM; d++) {
+			t.box.begin[d].raw() = s.box_begin[d];
+			t.box.end[d].raw() = s.box_end[d];
+			t.pos[d].raw() = s.pos[d];
+			mp[i].pos[d].raw() = s.pos[d];
+		}
+		t.children[LEFT].proc = t.children[RIGHT].proc = 0;
+		t.children[LEFT].index = s.child_left;
+		t.children[RIGHT].index = s.child_right;
+		t.part_range.first = s.part_begin;
+		t.part_range.second = s.part_end;
+		t.proc_range.first = 0;
+		t.proc_range.second = 1;
+		t.radius = s.radius;
+		t.depth = s.depth;
+		t.leaf = s.leaf ? 1 : 0;
+		t.local_root = i == 0;
+		for (int k = 0; k < MULTIPOLE_SIZE; k++) {
+			mp[i].multi[k] = s.multi[k];
+		}
+		t.mpos = mp + i;
+	}
+	*tn_out = tn;
+	*mp_out = mp;
+	return 0;
+}
+
+kick_params make_params(const void* pp);
+
 }  // namespace
 
 extern "C" {
@@ -206,6 +249,37 @@ typedef struct {
 	float a, t0, theta, h, eta, GM, max_dt;
 	int save_force, first_call, ascending, descending, top, do_phi;
 } ctref_kick_params;
+
+}  // extern "C"
+
+namespace {
+kick_params make_params(const void* pp) {
+	const ctref_kick_params* p = (const ctref_kick_params*) pp;
+	kick_params kp;
+	kp.sign = p->sign;
+	kp.min_level = 0;
+	kp.min_rung = p->min_rung;
+	kp.a = p->a;
+	kp.t0 = p->t0;
+	kp.theta = p->theta;
+	kp.h = p->h;
+	kp.eta = p->eta;
+	kp.GM = p->GM;
+	kp.vel_init = false;
+	kp.save_force = p->save_force != 0;
+	kp.first_call = p->first_call != 0;
+	kp.gpu = true;
+	kp.node_load = 0.f;
+	kp.max_dt = p->max_dt;
+	kp.ascending = p->ascending != 0;
+	kp.descending = p->descending != 0;
+	kp.top = p->top != 0;
+	kp.do_phi = p->do_phi != 0;
+	return kp;
+}
+}  // namespace
+
+extern "C" {
 
 // One-time set-up on the current device: the reference's device heap (cuda_mem_init, as
 // cuda_init does, src/cuda.cpp:99-110, with a caller-chosen size) and its Ewald tables in
@@ -240,58 +314,13 @@ int ctref_kick(int64_t n, const uint32_t* x, const uint32_t* y, const uint32_t* 
 		free_particles();
 		return -2;
 	}
-	tree_node* tn = managed<tree_node>(nnodes);
-	multi_pos* mp = managed<multi_pos>(nnodes);
-	if (!tn || !mp) {
+	tree_node* tn = nullptr;
+	multi_pos* mp = nullptr;
+	if (lay_out_tree(nnodes, nodes, &tn, &mp)) {
 		free_particles();
 		return -2;
 	}
-	for (int64_t i = 0; i < nnodes; i++) {
-		const ct_node& s = nodes[i];
-		tree_node& t = tn[i];
-		memset((void*) &t, 0, sizeof(t));
-		for (int d = 0; d < NDIM; d++) {
-			t.box.begin[d].raw() = s.box_begin[d];
-			t.box.end[d].raw() = s.box_end[d];
-			t.pos[d].raw() = s.pos[d];
-			mp[i].pos[d].raw() = s.pos[d];
-		}
-		t.children[LEFT].proc = t.children[RIGHT].proc = 0;
-		t.children[LEFT].index = s.child_left;
-		t.children[RIGHT].index = s.child_right;
-		t.part_range.first = s.part_begin;
-		t.part_range.second = s.part_end;
-		t.proc_range.first = 0;
-		t.proc_range.second = 1;
-		t.radius = s.radius;
-		t.depth = s.depth;
-		t.leaf = s.leaf ? 1 : 0;
-		t.local_root = i == 0;
-		for (int k = 0; k < MULTIPOLE_SIZE; k++) {
-			mp[i].multi[k] = s.multi[k];
-		}
-		t.mpos = mp + i;
-	}
-	kick_params kp;
-	kp.sign = p->sign;
-	kp.min_level = 0;
-	kp.min_rung = p->min_rung;
-	kp.a = p->a;
-	kp.t0 = p->t0;
-	kp.theta = p->theta;
-	kp.h = p->h;
-	kp.eta = p->eta;
-	kp.GM = p->GM;
-	kp.vel_init = false;
-	kp.save_force = p->save_force != 0;
-	kp.first_call = p->first_call != 0;
-	kp.gpu = true;
-	kp.node_load = 0.f;
-	kp.max_dt = p->max_dt;
-	kp.ascending = p->ascending != 0;
-	kp.descending = p->descending != 0;
-	kp.top = p->top != 0;
-	kp.do_phi = p->do_phi != 0;
+	const kick_params kp = make_params(p);
 	kick_workitem wi;
 	for (int k = 0; k < EXPANSION_SIZE; k++) {
 		wi.L[k] = 0.f;
@@ -305,6 +334,111 @@ int ctref_kick(int64_t n, const uint32_t* x, const uint32_t* y, const uint32_t* 
 	items.push_back(wi);
 	const kick_return kr = cuda_execute_kicks(kp, particles_x[XDIM], particles_x[YDIM], particles_x[ZDIM], tn, items);
 	cudaError_t e = cudaGetLastError();  // a failed launch is reported here, not by the sync
+	if (e == cudaSuccess) {
+		e = cudaDeviceSynchronize();
+	}
+	if (e == cudaSuccess) {
+		get_particles(n, nullptr, nullptr, nullptr, vxyz, rung);
+		if (p->save_force) {
+			for (int64_t i = 0; i < n; i++) {
+				gx[i] = particles_g[XDIM][i];
+				gy[i] = particles_g[YDIM][i];
+				gz[i] = particles_g[ZDIM][i];
+				pot[i] = particles_p[i];
+			}
+		}
+		ret[0] = kr.max_rung;
+		ret[1] = kr.pot;
+		ret[2] = kr.kin;
+		ret[3] = kr.dkin;
+		ret[4] = kr.xmom;
+		ret[5] = kr.ymom;
+		ret[6] = kr.zmom;
+		ret[7] = kr.nmom;
+	}
+	cudaFree(tn);
+	cudaFree(mp);
+	free_particles();
+	return e == cudaSuccess ? 0 : -3;
+}
+
+// Blocks of the reference's kick grid (kick_block_count, src/kick.cu:611-624: occupancy x
+// SMs); its CPU top hands the GPU subtrees of at most min(16384, max(active / this, bucket))
+// particles (kick.cpp:173-177).
+int ctref_kick_block_count() {
+	return g_ready ? kick_block_count() : -1;
+}
+
+// The reference's kick in its production form: cuda_execute_kicks (src/kick.cu:508-609) with
+// the caller's work items -- the subtrees below the CPU top of the walk, each with its parent
+// expansion, its centre and its direct and Ewald check lists (kick_workitem, kick.hpp:188-194;
+// made by kick() at kick.cpp:169-190 and ordered by first particle, kick_workspace.cpp:308-310)
+// -- on the caller's tree (ct_node layout; items index into it).  The kick runs `repeats` times
+// on the same particle copy (velocities and rungs advance each time); ms[r] receives each call's
+// time (CUDA events on the legacy default stream around the call: its host packing of the
+// items, the copy to the device, the kernel, the read-back of kick_return and its device
+// synchronisation).  Forces, potentials, velocities and rungs are those of the last call.
+int ctref_kick_items(int64_t n, const uint32_t* x, const uint32_t* y, const uint32_t* z, float* vxyz, int8_t* rung, int64_t nnodes,
+		const ct_node* nodes, const ctref_kick_params* p, int64_t nitems, const int32_t* self, const float* L, const uint32_t* pos,
+		const int64_t* doff, const int32_t* dlist, const int64_t* eoff, const int32_t* elist, int repeats, float* gx, float* gy, float* gz,
+		float* pot, double* ret, float* ms) {
+	if (!g_ready || n <= 0 || nnodes <= 0 || nitems <= 0 || repeats < 1) {
+		return -1;
+	}
+	if (set_particles(n, x, y, z, vxyz, rung, p->save_force != 0)) {
+		free_particles();
+		return -2;
+	}
+	tree_node* tn = nullptr;
+	multi_pos* mp = nullptr;
+	if (lay_out_tree(nnodes, nodes, &tn, &mp)) {
+		free_particles();
+		return -2;
+	}
+	const kick_params kp = make_params(p);
+	vector<kick_workitem> items(nitems);
+	for (int64_t i = 0; i < nitems; i++) {
+		kick_workitem& w = items[i];
+		for (int k = 0; k < EXPANSION_SIZE; k++) {
+			w.L[k] = L[i * EXPANSION_SIZE + k];
+		}
+		for (int d = 0; d < NDIM; d++) {
+			w.pos[d].raw() = pos[3 * i + d];
+		}
+		w.self.proc = 0;
+		w.self.index = self[i];
+		for (int64_t j = doff[i]; j < doff[i + 1]; j++) {
+			tree_id t;
+			t.proc = 0;
+			t.index = dlist[j];
+			w.dchecklist.push_back(t);
+		}
+		for (int64_t j = eoff[i]; j < eoff[i + 1]; j++) {
+			tree_id t;
+			t.proc = 0;
+			t.index = elist[j];
+			w.echecklist.push_back(t);
+		}
+	}
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	kick_return kr;
+	cudaError_t e = cudaSuccess;
+	for (int r = 0; r < repeats && e == cudaSuccess; r++) {
+		cudaEventRecord(e0, 0);
+		kr = cuda_execute_kicks(kp, particles_x[XDIM], particles_x[YDIM], particles_x[ZDIM], tn, items);
+		cudaEventRecord(e1, 0);
+		e = cudaGetLastError();
+		if (e == cudaSuccess) {
+			e = cudaEventSynchronize(e1);
+		}
+		if (e == cudaSuccess) {
+			cudaEventElapsedTime(ms + r, e0, e1);
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
 	if (e == cudaSuccess) {
 		e = cudaDeviceSynchronize();
 	}

@@ -211,6 +211,20 @@ class KickPlan:
             raise RuntimeError("oracle kick error %d" % err)
         return tuple(g), rc, flops.value, secs
 
+    def export(self, nexp=50):
+        """The items as the reference's kick_workitem fields: dict of self (int32), L (nitems,
+        nexp) float32, pos (nitems, 3) uint32, and the direct / Ewald check lists in CSR form
+        (doff, dlist, eoff, elist)."""
+        L_ = self.O.lib
+        nd, ne = ctypes.c_int64(0), ctypes.c_int64(0)
+        L_.ct_or_kick_plan_list_sizes(ctypes.c_void_p(self.h), ctypes.byref(nd), ctypes.byref(ne))
+        out = {"self": np.zeros(self.nitems, np.int32), "L": np.zeros((self.nitems, nexp), np.float32), "pos": np.zeros((self.nitems, 3), np.uint32),
+               "doff": np.zeros(self.nitems + 1, np.int64), "dlist": np.zeros(max(nd.value, 1), np.int32),
+               "eoff": np.zeros(self.nitems + 1, np.int64), "elist": np.zeros(max(ne.value, 1), np.int32)}
+        L_.ct_or_kick_plan_export(ctypes.c_void_p(self.h), _p(out["self"]), _p(out["L"]), ctypes.c_int(nexp), _p(out["pos"]), _p(out["doff"]),
+                                  _p(out["dlist"]), _p(out["eoff"]), _p(out["elist"]))
+        return out
+
     def particles(self, select):
         """Indices of the particles of the selected items."""
         idx = np.nonzero(select)[0]

@@ -208,11 +208,15 @@ def test_clustered256_tree_and_sampled_kick_parity(ctx, oracle):
     g_or = np.stack([gx[idx], gy[idx], gz[idx]], 1).astype(np.float64)
     ferr = rel_rms(g_gpu, g_or)
     perr = rel_rms(out["pot"][idx].astype(np.float64), pot[idx].astype(np.float64))
+    # potentials of the lattice particles are small residuals of the direct and Ewald sums
+    # (each about MEAN_INV_R_UNIT_CELL), so they are compared against that scale
+    pscale = float(np.sqrt(np.mean((out["pot"][idx].astype(np.float64) - pot[idx]) ** 2))) / MEAN_INV_R_UNIT_CELL
     verr = rel_rms(out["v"][idx].astype(np.float64), ovk[idx].astype(np.float64))
     nedge, ndiff = check_rungs(out["rung"][idx], ork[idx], g_gpu, g_or, okp, orr[idx])
-    print("clustered 256^3: %d sinks in %d work items; force rel rms %.3g, potential %.3g, velocity %.3g; rungs %s, boundary %d, differing %d"
-          % (len(idx), sel.sum(), ferr, perr, verr, np.bincount(out["rung"][idx]), nedge, ndiff))
-    assert ferr < KICK_RMS_TOL and perr < KICK_RMS_TOL and verr < KICK_RMS_TOL
+    print("clustered 256^3: %d sinks in %d work items; force rel rms %.3g, potential %.3g (/scale %.3g), velocity %.3g; rungs %s, boundary %d, differing %d"
+          % (len(idx), sel.sum(), ferr, perr, pscale, verr, np.bincount(out["rung"][idx]), nedge, ndiff))
+    assert ferr < KICK_RMS_TOL and verr < KICK_RMS_TOL
+    assert pscale < POT_SCALE_TOL
     assert ndiff <= max(2, len(idx) // 10000)
     assert kr.max_rung >= int(ork[idx].max())
 

@@ -134,3 +134,48 @@ def test_drift_matches_reference_cuda_drift(ctx, ref):
         assert moved > 0.2
         assert np.array_equal(out["x"], rx) and np.array_equal(out["y"], ry) and np.array_equal(out["z"], rz)
         box.close()
+
+
+def test_kick_matches_reference_production_work_items(ctx, ref, oracle):
+    """The reference's kick in its production form: the CPU top of the walk (the oracle's
+    restatement, kick.cpp:150-507 with kick.cu's list rules) hands the subtrees of at most
+    max_parts particles (kick.cpp:173-177) to cuda_execute_kicks as work items ordered by first
+    particle (kick_workspace.cpp:308-310); the reference's kernel then walks them on its
+    resident grid.  Same tree and particles as this project's kick: forces, potentials and
+    velocities within 1e-5 relative RMS, and the same rungs."""
+    import cosmictiger_b200 as ct
+    from tests import oracle_lib
+
+    x, y, z, v, r = ics.clustered_box(48, nspheres=int(round(20000 * (48 / 256) ** 3)), seed=7)
+    N = len(x)
+    theta = 0.55
+    h = ics.softening(N, 0.02)
+    eta = ics.eta_default()
+    nodes = oracle.tree_build(x, y, z, v, r, theta, h, 128)
+    box = ctx.box(N)
+    box.upload(x, y, z, v, r)
+    box.tree_create(theta, h, 128)
+    before = box.download()
+    assert np.array_equal(before["x"], x)  # already in tree order
+    t0 = 1.0 / 64
+    kr = box.kick(ct.KickParams.make(theta=theta, h=h, GM=1.0 / N, eta=eta, t0=t0, first_call=True, save_force=True))
+    out = box.download(forces=True)
+    box.close()
+    okp = oracle_lib.KickParams(sign=1.0, min_rung=0, a=1.0, t0=t0, theta=theta, h=h, eta=eta, GM=1.0 / N, max_dt=1e30, save_force=1, first_call=1,
+                                ascending=1, descending=1, top=1, do_phi=1)
+    plan = oracle.plan(okp, nodes, x, y, z, max_parts=ref.max_parts(N))
+    items = plan.export()
+    plan.close()
+    assert len(items["self"]) > 100
+    rp = rg.RefKickParams(sign=1.0, min_rung=0, a=1.0, t0=t0, theta=theta, h=h, eta=eta, GM=1.0 / N, max_dt=1e30, save_force=1, first_call=1,
+                          ascending=1, descending=1, top=1, do_phi=1)
+    ro = ref.kick_items(before, nodes, rp, items, repeats=1)
+    ferr = rel_rms(forces(out), forces(ro))
+    perr = rel_rms(out["pot"].astype(np.float64), ro["pot"].astype(np.float64))
+    verr = rel_rms(out["v"].astype(np.float64), ro["v"].astype(np.float64))
+    rdiff = int(np.sum(out["rung"] != ro["rung"]))
+    print("vs reference CUDA kick on %d work items (clustered 48^3): force rel rms %.3g, potential %.3g, velocity %.3g, rungs differing %d, %.2f ms"
+          % (len(items["self"]), ferr, perr, verr, rdiff, ro["ms"][0]))
+    assert ferr < KICK_RMS_TOL and perr < KICK_RMS_TOL and verr < KICK_RMS_TOL
+    assert rdiff <= 2
+    assert kr.max_rung == ro["max_rung"]
