@@ -646,7 +646,7 @@ def cpu_summary(args, N, runs, frac, wall_s, forces="the device's"):
             "sample": "%s: one hierarchical step (the same ladder of rung sorts, tree builds over the active particles, kicks and drifts as the "
                       "device step; %d kicks, %.2e active kicks) per repeat; tree builds (%d threads), the top of each walk, sorts and drifts run in "
                       "full; of %d work items below the top, %d were walked (chosen with probability proportional to a cost proxy, %.0f%% of it "
-                      "covered) and the walk of all items estimated from them (Horvitz-Thompson); starting rungs from %s forces by the rung rule"
+                      "covered) and the walk of all items estimated from them (Horvitz-Thompson total, thread schedule simulated); starting rungs from %s forces by the rung rule"
                       % (workload_name(args), est["kicks"], est["active"], est["threads"], est["items"], est["sampled_items"], 100 * frac, forces)}
 
 

@@ -498,48 +498,91 @@ __global__ void __launch_bounds__(128, 3) k_m2l_ewald(int64_t nn, const NodeW* _
 	}
 }
 
-// Direct M2L: dL += sum over the direct CC list.
+// Asynchronous 16-byte global -> shared copies (cp.async; L1-allocating, the multipoles of
+// a source node are read by many sink nodes): one group per stage, waited for per thread.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+	const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+	asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template<int N>
+__device__ __forceinline__ void cp_async_wait() {
+	asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Shared memory of k_m2l_direct: per warp the 32 lanes' expansion rows (51 floats: lanes on
+// distinct banks) and two stages of one source per lane (its centre and radius, 16 bytes, and
+// its multipole row, 160 bytes).
+constexpr int M2L_STAGE = 44;  // floats per lane and stage
+constexpr size_t M2L_DIRECT_SMEM = sizeof(float) * (4 * 32 * 51 + 4 * 2 * 32 * M2L_STAGE);
+
+// Direct M2L: dL += sum over the direct CC list (gravity.cu:44-73).  Lanes take the sources
+// 32 apart; each lane copies its next source (centre and multipole) into shared memory while
+// it evaluates the current one, so that the gathers from global memory overlap the arithmetic.
 template<class Ops>
 __global__ void __launch_bounds__(128, 3) k_m2l_direct(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi,
 		const int2* __restrict__ dcc, const int* __restrict__ dcc_list, float* __restrict__ dL, int do_phi) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
-	__shared__ float s_L[4][32][51];
-	const int lane = threadIdx.x & 31;
+	extern __shared__ __align__(16) float m2l_smem[];
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	float* s_L = m2l_smem;  // [4][32][51]
+	float* my_stage = m2l_smem + 4 * 32 * 51 + ((w * 2) * 32 + lane) * M2L_STAGE;  // stage b at + b * 32 * M2L_STAGE
 	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int nw = (gridDim.x * blockDim.x) >> 5;
+	auto stage = [&](int c, int b) {
+		float* d = my_stage + b * 32 * M2L_STAGE;
+		cp_async16(d, nodes + c);
+		const float* mp = multi + (size_t) NMULT_STRIDE * c;
+#pragma unroll
+		for (int k = 0; k < (NM + 3) / 4; k++) {
+			cp_async16(d + 4 + 4 * k, mp + 4 * k);
+		}
+	};
 	for (int64_t si = gw; si < nn; si += nw) {
 		const int2 lst = dcc[si];
 		if (lst.y == 0) {
 			continue;
 		}
 		const NodeW self = nodes[si];
-		// this lane's expansion sum in shared memory (rows of 51 floats: lanes on distinct banks)
-		float* L = &s_L[threadIdx.x >> 5][lane][0];
+		float* L = s_L + (w * 32 + lane) * 51;
 		for (int i = 0; i < NE; i++) {
 			L[i] = 0.f;
 		}
+		int b = 0;
+		if (lane < lst.y) {
+			stage(dcc_list[lst.x + lane], 0);
+		}
+		cp_async_commit();
 		for (int j = lane; j < lst.y; j += 32) {
-			const int c = dcc_list[lst.x + j];
-			const NodeW ot = nodes[c];
+			if (j + 32 < lst.y) {
+				stage(dcc_list[lst.x + j + 32], b ^ 1);
+			}
+			cp_async_commit();
+			cp_async_wait<1>();  // this stage's copies (all but the group just committed)
+			const float* d = my_stage + b * 32 * M2L_STAGE;
+			const uint4 oc = *(const uint4*) d;
 			float M[NM], D[NE];
-			const float4* mp = (const float4*) (multi + (size_t) NMULT_STRIDE * c);
 #pragma unroll
 			for (int k = 0; k < (NM + 3) / 4; k++) {
-				const float4 v = __ldg(mp + k);
+				const float4 v = *(const float4*) (d + 4 + 4 * k);
 				if (4 * k + 0 < NM) M[4 * k + 0] = v.x;
 				if (4 * k + 1 < NM) M[4 * k + 1] = v.y;
 				if (4 * k + 2 < NM) M[4 * k + 2] = v.z;
 				if (4 * k + 3 < NM) M[4 * k + 3] = v.w;
 			}
-			Ops::greens(D, fixed_dist(self.x, ot.x), fixed_dist(self.y, ot.y), fixed_dist(self.z, ot.z));
+			Ops::greens(D, fixed_dist(self.x, oc.x), fixed_dist(self.y, oc.y), fixed_dist(self.z, oc.z));
 			Ops::m2l(L, M, D, do_phi != 0);
+			b ^= 1;
 		}
+		cp_async_wait<0>();
 		__syncwarp();
 		// entry n summed over the 32 lanes' rows by lane n % 32
 		for (int n = lane; n < NE; n += 32) {
 			float t = 0.f;
 			for (int q = 0; q < 32; q++) {
-				t += s_L[threadIdx.x >> 5][q][n];
+				t += s_L[(w * 32 + q) * 51 + n];
 			}
 			dL[NEXP_STRIDE * si + n] += t;
 		}
@@ -584,34 +627,36 @@ __global__ void __launch_bounds__(128) k_p2l(int64_t nn, const NodeW* __restrict
 				inc += lane >= o ? t : 0;
 			}
 			const int total = __shfl_sync(0xffffffffu, inc, 31);
-			const int first = beg - (inc - cnt);  // particle index = first[owner] + flat index
+			const int start = inc - cnt;  // this lane's leaf: flat indices [start, inc)
+			const int first = beg - start;  // particle index = first[owner] + flat index
 			ncp += total;
-			// owner lane of flat index g: the number of lanes whose inclusive prefix is <= g
-			auto particle = [&](int g) {
-				int l = 0;
-#pragma unroll
-				for (int s = 16; s; s >>= 1) {
-					l += __shfl_sync(0xffffffffu, inc, l + s - 1) <= g ? s : 0;
-				}
-				return __shfl_sync(0xffffffffu, first, l) + g;
+			// particle of flat index gb + lane: the leaves ending at or before gb (one ballot)
+			// plus the leaves starting inside (gb, gb + lane] (one OR-reduction of start bits)
+			// give the owner lane (leaves holding particles start at distinct flat indices)
+			auto particle = [&](int gb) {
+				const int o0 = __popc(__ballot_sync(0xffffffffu, inc <= gb));
+				const int rel = start - gb;
+				const unsigned starts = __reduce_or_sync(0xffffffffu, (cnt > 0 && rel > 0 && rel < 32) ? (1u << rel) : 0u);
+				const int owner = o0 + __popc(starts & ((2u << lane) - 1u));
+				return __shfl_sync(0xffffffffu, first, owner & 31) + gb + lane;
 			};
-			int g = lane;
-			int k = particle(g);
+			int k = particle(0);
 			uint32_t px = 0, py = 0, pz = 0;
-			if (g < total) {
+			if (lane < total) {
 				px = x0[k];
 				py = x1[k];
 				pz = x2[k];
 			}
 			for (int gb = 0; gb < total; gb += 32) {
 				const uint32_t cx = px, cy = py, cz = pz;
-				const bool have = g < total;
-				g += 32;
-				k = particle(g);
-				if (g < total) {
-					px = x0[k];
-					py = x1[k];
-					pz = x2[k];
+				const bool have = gb + lane < total;
+				if (gb + 32 < total) {
+					k = particle(gb + 32);
+					if (gb + 32 + lane < total) {
+						px = x0[k];
+						py = x1[k];
+						pz = x2[k];
+					}
 				}
 				if (have) {
 					Ops::greens_add(L, fixed_dist(self.x, cx), fixed_dist(self.y, cy), fixed_dist(self.z, cz));
@@ -1430,7 +1475,8 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		c->launches++;
 		k_m2l_ewald<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL, kp->do_phi, counters);
 		c->launches++;
-		k_m2l_direct<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, K.dL, kp->do_phi);
+		CT_CUDA(c, cudaFuncSetAttribute(k_m2l_direct<Ops>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) M2L_DIRECT_SMEM));
+		k_m2l_direct<Ops><<<gm, 128, M2L_DIRECT_SMEM, st>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, K.dL, kp->do_phi);
 		c->launches++;
 		k_p2l<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL, counters);
 		cudaEventRecord(c->ev[2], st);

@@ -254,8 +254,7 @@ def gen_greens(P, accumulate=False):
     stored = tl_stored(P)
     em("x *= T(%g); y *= T(%g); z *= T(%g);" % (SCALE, SCALE, SCALE))
     em("const T r2 = ct_fma(x, x, ct_fma(y, y, z * z));")
-    em("const T r = ct_sqrt(r2);")
-    em("const T rinv = r > T(0) ? T(1) / r : T(0);")
+    em("const T rinv = ct_rinv(r2);")
     em("const T ux = x * rinv, uy = y * rinv, uz = z * rinv;")
     needed = set()
     for n in stored:

@@ -337,13 +337,35 @@ def item_proxy(plan):
     return plan.nparts.astype(np.float64) * (plan.near_parts.astype(np.float64) + 64.0) + 4000.0 * plan.ewald_checks
 
 
+def walk_makespan(proxy, mask, pi, secs, nthreads):
+    """Estimated wall time of walking all items on nthreads threads that take items in order
+    from a shared counter (the oracle's parallel_for): the sampled items' measured times, the
+    others' predicted from their cost proxy (ratio estimator), the greedy schedule simulated,
+    and scaled so that the items' total equals the unbiased Horvitz-Thompson total."""
+    import heapq
+
+    proxy = np.maximum(np.asarray(proxy, np.float64), 1.0)
+    total = float(np.sum(secs[mask] / pi[mask]))
+    if total <= 0.0:
+        return 0.0
+    rest = proxy[~mask].sum()
+    beta = (total - secs[mask].sum()) / rest if rest > 0 else 0.0
+    t = np.where(mask, secs, max(beta, 0.0) * proxy)
+    busy = [0.0] * nthreads
+    for ti in t:
+        heapq.heappush(busy, heapq.heappop(busy) + ti)
+    span = max(busy)
+    return span * total / max(float(t.sum()), 1e-300)
+
+
 def estimate_step_hierarchical(O, st, sp, frac, seed, order=7, nthreads=0, max_parts=None):
     """One hierarchical step of the oracle (the ladder of step_hierarchical above, on state `st`)
     with every kick timed on a sample: the tree build over the active particles, the top of the
     walk and the rung sort and drift run in full; of the work items below the top a random
     subset is walked, chosen with probability proportional to a cost proxy, and the walk time
-    of all items is estimated from it (Horvitz-Thompson: sum of t_i / pi_i over the sample,
-    divided by the threads).  Returns (estimated seconds, details); the state advances as the
+    of all items is estimated from it (the Horvitz-Thompson total, sum of t_i / pi_i over the
+    sample, spread over the threads by walk_makespan's simulation of their schedule).
+    Returns (estimated seconds, details); the state advances as the
     step moves it (unsampled particles keep their rungs and velocities)."""
     import time
 
@@ -391,7 +413,7 @@ def estimate_step_hierarchical(O, st, sp, frac, seed, order=7, nthreads=0, max_p
         mask, pi = pps_select(item_proxy(plan), frac, rng, min_items=2 * nthreads)
         _, kr, _, secs = plan.run(v, r, select=mask, save_force=False)
         plan.close()
-        est["walk"] += float(np.sum(secs[mask] / pi[mask])) / nthreads
+        est["walk"] += walk_makespan(item_proxy(plan), mask, pi, secs, nthreads)
         est["walk_sampled"] += float(np.sum(secs[mask]))
         est["kicks"] += 1
         est["active"] += active
