@@ -528,6 +528,17 @@ ct_status ct_ctx_create(ct_ctx** out, int device, size_t hbm_budget_bytes, int o
 	for (int i = 0; i < 16; i++) {
 		cudaEventCreate(&c->ev[i]);
 	}
+	for (int i = 0; i < 2; i++) {
+		if (cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking) != cudaSuccess ||
+				cudaEventCreateWithFlags(&c->join_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+			ct_ctx_destroy((ct_ctx*) c);
+			return CT_ERR_CUDA;
+		}
+	}
+	if (cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming) != cudaSuccess) {
+		ct_ctx_destroy((ct_ctx*) c);
+		return CT_ERR_CUDA;
+	}
 	c->pinned_bytes = 1 << 16;
 	if (cudaMallocHost(&c->pinned, c->pinned_bytes) != cudaSuccess) {
 		delete c;
@@ -572,6 +583,18 @@ void ct_ctx_destroy(ct_ctx* ctx) {
 	}
 	for (int i = 0; i < 16; i++) {
 		cudaEventDestroy(c->ev[i]);
+	}
+	for (int i = 0; i < 2; i++) {
+		if (c->side[i]) {
+			cudaStreamSynchronize(c->side[i]);
+			cudaStreamDestroy(c->side[i]);
+		}
+		if (c->join_ev[i]) {
+			cudaEventDestroy(c->join_ev[i]);
+		}
+	}
+	if (c->fork_ev) {
+		cudaEventDestroy(c->fork_ev);
 	}
 	if (c->stream) {
 		cudaStreamSynchronize(c->stream);

@@ -152,6 +152,10 @@ struct Ctx {
 	double* d_counters = nullptr; // interaction counters
 	void* d_ewald_tab = nullptr;  // device copy of the Ewald tables (when not in __constant__)
 	cudaEvent_t ev[16];
+	// two more streams for the kick's M2L phase, whose three kernels (Ewald M2L, direct M2L,
+	// P2L) run side by side: forked from `stream` by fork_ev and joined back by join_ev
+	cudaStream_t side[2] = { nullptr, nullptr };
+	cudaEvent_t fork_ev = nullptr, join_ev[2] = { nullptr, nullptr };
 	bool drift_timed = false;         // ev[6], ev[7] hold a recorded drift
 	unsigned long long launches = 0;  // kernels of this library launched so far
 	int compensated = 1;              // Neumaier-compensated P2P batch sums

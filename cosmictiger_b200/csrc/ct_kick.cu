@@ -678,11 +678,14 @@ __global__ void __launch_bounds__(128) k_p2l(int64_t nn, const NodeW* __restrict
 // ---------------------------------------------------------------- L2L (top-down, one level)
 template<class Ops>
 __global__ void k_l2l(int64_t lb, int64_t le, const NodeW* __restrict__ nodes, const int32_t* __restrict__ parent, const float* __restrict__ dL,
-		float* __restrict__ Lx, int do_phi) {
+		const float* __restrict__ dL2, const float* __restrict__ dL3, float* __restrict__ Lx, int do_phi) {
 	constexpr int NE = Ops::NEXP;
 	for (int64_t i = lb + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < le; i += (int64_t) gridDim.x * blockDim.x) {
-		float out[NE];
-		const float* d = dL + NEXP_STRIDE * i;
+		float out[NE], d[NE];
+		// the node's M2L and P2L sums, added in the order one stream would add them
+		for (int k = 0; k < NE; k++) {
+			d[k] = (dL[NEXP_STRIDE * i + k] + dL2[NEXP_STRIDE * i + k]) + dL3[NEXP_STRIDE * i + k];
+		}
 		if (parent[i] < 0) {  // a root: the expansion starts at zero
 			for (int k = 0; k < NE; k++) {
 				out[k] = d[k];
@@ -1113,7 +1116,7 @@ struct KickTileArgs {
 // Sums of the kick return go to one set per box: block-reduced for a single box, per tile
 // (warp-reduced, atomically added to the tile's box) for an ensemble.
 template<class Ops>
-__global__ void __launch_bounds__(128) k_leaf_kick(KickTileArgs a) {
+__global__ void __launch_bounds__(128, 3) k_leaf_kick(KickTileArgs a) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
 	__shared__ double s_red[4][9];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1352,8 +1355,12 @@ struct KickBuffers {
 	size_t stage_n = 0;
 	int stage_cap = 0;
 	int nwarps = 0;
-	float* dL = nullptr;
+	float* dL = nullptr;  // Ewald M2L sums (then L2L adds the next two)
 	size_t dL_n = 0;
+	float* dL2 = nullptr;  // direct M2L sums
+	size_t dL2_n = 0;
+	float* dL3 = nullptr;  // P2L sums
+	size_t dL3_n = 0;
 	float* Lx = nullptr;
 	size_t Lx_n = 0;
 	int64_t* leaves = nullptr;
@@ -1394,6 +1401,8 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 	// per-node list descriptors
 	CT_TRY(ensure(c, &K.per_node, K.per_node_n, (size_t) 7 * nn, "walk descriptors"));
 	CT_TRY(ensure(c, &K.dL, K.dL_n, (size_t) NEXP_STRIDE * nn, "expansion deltas"));
+	CT_TRY(ensure(c, &K.dL2, K.dL2_n, (size_t) NEXP_STRIDE * nn, "expansion deltas (direct M2L)"));
+	CT_TRY(ensure(c, &K.dL3, K.dL3_n, (size_t) NEXP_STRIDE * nn, "expansion deltas (P2L)"));
 	CT_TRY(ensure(c, &K.Lx, K.Lx_n, (size_t) NEXP_STRIDE * nn, "local expansions"));
 	CT_TRY(ensure(c, &K.leaves, K.leaves_n, (size_t) nn, "leaf index"));
 	K.nwarps = c->nsm * 16 * (WALK_TPB / 32) / 4;  // 4 blocks of 4 warps per SM
@@ -1471,20 +1480,34 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		CT_CUDA(c, cudaMemsetAsync(counters, 0, 16 * sizeof(double), st));
 		// node-indexed kernels: a static interleave over all nodes (most hold no list of the
 		// kind; a work counter costs more here than the last wave's tail)
+		// The three kernels run side by side on three streams, each into its own expansion
+		// deltas; L2L adds them in this order, dL + dL2 + dL3, the order of one stream.
 		const int gm = c->nsm * 8;
+		const size_t dl_bytes = sizeof(float) * NEXP_STRIDE * nn;
+		CT_CUDA(c, cudaEventRecord(c->fork_ev, st));
+		for (int k = 0; k < 2; k++) {
+			CT_CUDA(c, cudaStreamWaitEvent(c->side[k], c->fork_ev, 0));
+		}
 		c->launches++;
 		k_m2l_ewald<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL, kp->do_phi, counters);
+		CT_CUDA(c, cudaMemsetAsync(K.dL2, 0, dl_bytes, c->side[0]));
 		c->launches++;
 		CT_CUDA(c, cudaFuncSetAttribute(k_m2l_direct<Ops>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) M2L_DIRECT_SMEM));
-		k_m2l_direct<Ops><<<gm, 128, M2L_DIRECT_SMEM, st>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, K.dL, kp->do_phi);
+		k_m2l_direct<Ops><<<gm, 128, M2L_DIRECT_SMEM, c->side[0]>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, K.dL2, kp->do_phi);
+		CT_CUDA(c, cudaMemsetAsync(K.dL3, 0, dl_bytes, c->side[1]));
 		c->launches++;
-		k_p2l<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL, counters);
+		k_p2l<Ops><<<gm, 128, 0, c->side[1]>>>(nn, b->nodes, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL3, counters);
+		for (int k = 0; k < 2; k++) {
+			CT_CUDA(c, cudaEventRecord(c->join_ev[k], c->side[k]));
+			CT_CUDA(c, cudaStreamWaitEvent(st, c->join_ev[k], 0));
+		}
 		cudaEventRecord(c->ev[2], st);
 		for (int k = 0; k < nlev; k++) {
 			const int64_t lb = b->level_start[k], le = b->level_start[k + 1];
 			const int64_t g = (le - lb + 127) / 128;
 			c->launches++;
-			k_l2l<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>(g, c->nsm * 16)), 128, 0, st>>>(lb, le, b->nodes, b->parent, K.dL, K.Lx, kp->do_phi);
+			k_l2l<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>(g, c->nsm * 16)), 128, 0, st>>>(lb, le, b->nodes, b->parent, K.dL, K.dL2, K.dL3,
+					K.Lx, kp->do_phi);
 		}
 		cudaEventRecord(c->ev[3], st);
 		// leaves
@@ -1698,6 +1721,8 @@ void kick_buffers_release(Ctx* c) {
 	dfree(c, K->pass, sizeof(int) * K->pass_n);
 	dfree(c, K->stage, sizeof(int) * K->stage_n);
 	dfree(c, K->dL, sizeof(float) * K->dL_n);
+	dfree(c, K->dL2, sizeof(float) * K->dL2_n);
+	dfree(c, K->dL3, sizeof(float) * K->dL3_n);
 	dfree(c, K->Lx, sizeof(float) * K->Lx_n);
 	dfree(c, K->leaves, sizeof(int64_t) * K->leaves_n);
 	delete K;
