@@ -52,12 +52,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own CUDA kick on the same box")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape instead of autotuning it first")
     ap.add_argument("--accuracy-sinks", type=int, default=10000, help="FP64 direct-Ewald check on this many seeded sinks (0: skip)")
     ap.add_argument("--ensemble-boxes", type=int, default=64, help="boxes of the batched-vs-plain ensemble comparison (0: skip)")
     ap.add_argument("--ensemble-nmin", type=int, default=16)
     ap.add_argument("--ensemble-nmax", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=3)
-    ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving", "lightcone", "fourier"],
+    ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving", "lightcone", "fourier", "autotune"],
                     help="instead of the benchmark line: precision (theta x order x summation, force error vs FP64 Ewald and "
                          "particle-steps/s), ensemble (512 boxes of 16^3..128^3, batched vs box by box, 20 steps) or serving "
                          "(Poisson arrivals of 32^3..256^3 requests, rate sweep, p50/p99 latency vs sequential runs) or lightcone "
@@ -251,6 +252,16 @@ def main():
     eta = ics.eta_default()
     t0 = 1.0 / 64
     ctx = ct.Context(device=local, order=7)
+    tuning = None
+    if not args.no_tune:
+        # the kick's launch shape (P2P cell-list size, warps per sink tile, sink tile width)
+        # tuned on this workload at the benchmark's leaf size; results change only by rounding
+        from cosmictiger_b200 import autotune
+
+        tr = autotune.tune(ctx, (x, y, z, v, r), theta=args.theta, h=ics.softening(N, 0.02), buckets=(128,), max_force_rms=1e-5, repeats=1)
+        tuning = {"chosen": {k: tr["best"][k] for k in ("p2p_stage", "warps_per_tile", "tile_width")}, "ms_kick_chosen": tr["best"]["ms"],
+                  "ms_kick_default": tr["reference"]["ms"], "candidates": len(tr["rows"]), "by": "cosmictiger_b200.autotune.tune (device time of "
+                  "one all-particles tree build + kick per candidate)"}
     box = ctx.box(N)
     box.upload(x, y, z, v, r)
 
@@ -486,6 +497,7 @@ def main():
             "dtype": "f32 (fixed32 positions, f64 tree geometry)",
             "data": "synthetic (seeded generator)",
             "config": {"workload": workload_name(args), "particles_per_gpu": N, "theta": theta, "order": 7, "bucket": 128,
+                       "launch_shape": tuning if tuning else ctx.tuning(),
                        "parallelism": "independent boxes per GPU" if world > 1 else "single box",
                        "l2": "inputs larger than L2 (%.0f MB of particle state)" % (N * 41 / 1e6)},
             "e2e": e2e,
@@ -1073,6 +1085,41 @@ def study_fourier(args, torch):
                              "cores": 1, "kind": "port", "sample": "numpy restatement on %d^3" % m}}
 
 
+def study_autotune(args, torch):
+    """The autotuner's joint search (leaf size x launch shape) on the benchmark box (clustered,
+    n^3, theta 0.55) and on a batched ensemble of the C4 kind (boxes of 16^3..128^3); every
+    candidate's device time and force difference from the default (leaf 128, shape 128/1/32)."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import autotune, ics
+
+    out = {}
+    ctx = ct.Context(order=7)
+    state = make_ics(args, seed=3)
+    N = len(state[0])
+    res = autotune.tune(ctx, state, theta=args.theta, h=ics.softening(N, 0.02), buckets=(64, 96, 128, 160, 192), max_force_rms=None, repeats=2)
+    out["single_box"] = {"workload": workload_name(args).replace("4-rung hierarchical steps", "all-particles kick"), **res}
+    print(json.dumps({"single_box_best": res["best"], "reference": res["reference"]}), flush=True)
+    nb = args.ensemble_boxes if args.ensemble_boxes != 64 else 128
+    sets = make_ensemble(nb, 16, 128, seed=4)
+    counts = [len(s[0]) for s in sets]
+    cat = [np.concatenate([s[k] for s in sets]) for k in range(5)]
+    hs = np.array([ics.softening(n, 0.02) for n in counts], np.float32)
+    gms = np.array([1.0 / n for n in counts], np.float32)
+
+    def factory():
+        e = ctx.ensemble(counts)
+        e.upload(*cat)
+        e.set_box_params(hs, gms)
+        return e
+
+    res2 = autotune.tune(ctx, cat, theta=args.theta, h=float(hs.max()), buckets=(64, 96, 128, 160, 192), max_force_rms=None, repeats=2,
+                         box_factory=factory)
+    out["ensemble"] = {"boxes": nb, "particles": int(sum(counts)), "n_range": [16, 128], **res2}
+    print(json.dumps({"ensemble_best": res2["best"], "reference": res2["reference"]}), flush=True)
+    ctx.close()
+    return {"study": "autotune", **out}
+
+
 def peaks_hbm():
     try:
         with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
@@ -1085,7 +1132,8 @@ def run_study(args):
     import torch
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    fn = {"precision": study_precision, "ensemble": study_ensemble, "serving": study_serving, "lightcone": study_lightcone, "fourier": study_fourier}[args.study]
+    fn = {"precision": study_precision, "ensemble": study_ensemble, "serving": study_serving, "lightcone": study_lightcone, "fourier": study_fourier,
+          "autotune": study_autotune}[args.study]
     t = time.perf_counter()
     res = fn(args, torch)
     res["wall_s"] = time.perf_counter() - t

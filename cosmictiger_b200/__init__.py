@@ -90,6 +90,12 @@ class StepReturn(ctypes.Structure):
                 ("particles_drifted_levels", ctypes.c_int)]
 
 
+class Tuning(ctypes.Structure):
+    """Mirror of ct_tuning: P2P cell-list size, warps per sink tile, sinks per tile."""
+
+    _fields_ = [("p2p_stage", ctypes.c_int), ("warps_per_tile", ctypes.c_int), ("tile_width", ctypes.c_int)]
+
+
 class Counters(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "pp_pairs", "cc_direct", "cc_ewald", "cp_pairs", "pc_pairs", "nodes", "leaves", "flops", "flops_pp", "flops_cc",
@@ -190,6 +196,8 @@ def library():
     L.ct_stream.argtypes = [vp]
     L.ct_stream.restype = vp  # a cudaStream_t: a 64-bit handle, not an int
     L.ct_fp32_peak.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    L.ct_ctx_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.ct_ctx_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.ct_sort_by_rung_noalloc.argtypes = [i64, i64, i32, vp, vp, vp, vp, vp, vp, vp, ctypes.POINTER(i64), vp]
     L.ct_direct_ewald.argtypes = [vp, i32, i64, vp, vp, vp, ctypes.c_double, vp, vp, vp, vp]
     L.ct_drift_lightcone.argtypes = [vp, i32, i32, ctypes.c_float, ctypes.c_float, ctypes.c_double, ctypes.POINTER(LcParams), ctypes.POINTER(i64)]
@@ -236,6 +244,16 @@ class Context:
     def launches(self):
         """Kernels of libct_gravity launched on this context so far."""
         return int(self.lib.ct_launch_count(self.h))
+
+    def set_tuning(self, p2p_stage=128, warps_per_tile=1, tile_width=32):
+        """Launch shape of the P2P and leaf-kick kernels (ct_ctx_set_tuning)."""
+        t = Tuning(p2p_stage, warps_per_tile, tile_width)
+        self.check(self.lib.ct_ctx_set_tuning(self.h, ctypes.byref(t)), "ct_ctx_set_tuning")
+
+    def tuning(self):
+        t = Tuning()
+        self.check(self.lib.ct_ctx_get_tuning(self.h, ctypes.byref(t)), "ct_ctx_get_tuning")
+        return {"p2p_stage": t.p2p_stage, "warps_per_tile": t.warps_per_tile, "tile_width": t.tile_width}
 
     def set_compensated(self, on):
         """Neumaier-compensated (True, default) or plain FP32 sums of the P2P source batches."""

@@ -1,10 +1,19 @@
-"""Leaf-size tuning for a workload.
+"""Autotuning of the kick's launch shape and leaf size for a workload.
 
-The kick kernels' sink tile (32 sinks per warp, 16 or fewer in the small-tile launch) and the
-warps per tile are fixed when the library is built; the leaf size -- the tree's bucket, the
-reference's `bucket_size` option passed to tree_create (src/tree.cpp:273) -- is the run-time
-knob.  Larger leaves move work from the multipole operators (M2L, P2L, M2P, tree depth) to
-direct particle pairs; the best size depends on the clustering and on theta.
+The knobs (the reference fixes all of them at build time):
+  * the leaf size -- the tree's bucket, the reference's `bucket_size` option passed to
+    tree_create (src/tree.cpp:273); larger leaves move work from the multipole operators (M2L,
+    P2L, M2P, tree depth) to direct particle pairs, and change the forces within the
+    expansion's truncation error;
+  * the P2P cell-list size -- source particles staged in shared memory per pass (the
+    reference's KICK_PP_MAX, cosmictiger/kick.hpp:48): 64, 128 or 256;
+  * warps per sink tile -- one warp, or a pair splitting the tile's sources: 1 or 2;
+  * sink tile width -- sinks per tile for P2P and the leaf kick: 32, or 16 (each sink's
+    sources and multipoles then spread over two or more lanes).
+The last three change only the order of the per-sink sums (ct_ctx_set_tuning).
+
+tune() times every (leaf size, launch shape) pair on a representative state and returns the
+fastest whose forces stay within `max_force_rms` of the reference configuration's.
 
 tune_bucket times every candidate on a representative state with the library's own device
 timings of the phases (tree build, walk, M2L, L2L, P2P, leaf kick; the kick changes velocities
@@ -68,3 +77,55 @@ def tune_bucket(ctx, state, theta=0.55, h=None, candidates=(64, 96, 128, 160, 19
     ok = [row for row in rows if not check or row["force_rms"] <= max_force_rms]
     best = min(ok, key=lambda row: row["ms"])["bucket"]
     return {"best": best, "rows": sorted(rows, key=lambda row: row["bucket"])}
+
+
+SHAPES = tuple((s, w, t) for s in (64, 128, 256) for w in (1, 2) for t in (32, 16))
+
+
+def tune(ctx, state, theta=0.55, h=None, buckets=(128,), shapes=SHAPES, reference=(128, (128, 1, 32)), max_force_rms=1e-5, repeats=2,
+         box_factory=None):
+    """Joint search over leaf sizes and launch shapes (p2p_stage, warps_per_tile, tile_width).
+    Every candidate runs repeats + 1 times (the first untimed) on the state uploaded again each
+    time; the time is the library's device time of the kick's phases (tree build included).
+    Forces are compared with the reference candidate's (particles matched by position);
+    max_force_rms None keeps every candidate.  box_factory() (default ctx.box(n)) makes the box
+    the candidates run on, e.g. an ensemble with its per-box parameters set.  Leaves the context at the chosen shape; returns
+    {"best": {...}, "reference": {...}, "rows": [...]}."""
+    from . import KickParams
+
+    if repeats < 1:
+        raise ValueError("repeats must be >= 1 (the first run of each candidate is not timed)")
+    x, y, z, v, r = state
+    n = len(x)
+    h = ics.softening(n, 0.02) if h is None else h
+    cands = [(b, sh) for b in buckets for sh in shapes]
+    if reference in cands:
+        cands.remove(reference)
+    cands = [reference] + cands
+    box = box_factory() if box_factory else ctx.box(n)
+    rows = []
+    ref = None
+    try:
+        for bucket, shape in cands:
+            ctx.set_tuning(*shape)
+            times = []
+            g = None
+            for rep in range(repeats + 1):
+                box.upload(x, y, z, v, r)
+                box.tree_create(theta, h, bucket)
+                box.kick(KickParams.make(theta=theta, h=h, GM=1.0 / n, eta=ics.eta_default(), t0=1.0 / 64, first_call=True, save_force=True))
+                c = box.counters()
+                if rep > 0:
+                    times.append(sum(c[p] for p in PHASES))
+                if rep == repeats:
+                    g = _by_position(box.download(forces=True))
+            if ref is None:
+                ref = g
+            rows.append({"bucket": bucket, "p2p_stage": shape[0], "warps_per_tile": shape[1], "tile_width": shape[2], "ms": float(min(times)),
+                         "force_rms": float(np.sqrt(np.sum((g - ref) ** 2) / np.sum(ref ** 2)))})
+    finally:
+        box.close()
+    ok = [row for row in rows if max_force_rms is None or row["force_rms"] <= max_force_rms]
+    best = min(ok, key=lambda row: row["ms"])
+    ctx.set_tuning(best["p2p_stage"], best["warps_per_tile"], best["tile_width"])
+    return {"best": best, "reference": rows[0], "rows": rows}

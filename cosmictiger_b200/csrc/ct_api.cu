@@ -1227,6 +1227,29 @@ ct_status ct_ctx_set_compensated(ct_ctx* ctx, int compensated) {
 	return CT_OK;
 }
 
+ct_status ct_ctx_set_tuning(ct_ctx* ctx, const ct_tuning* t) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c || !t) {
+		return CT_ERR_ARG;
+	}
+	const bool ok = (t->p2p_stage == 64 || t->p2p_stage == 128 || t->p2p_stage == 256) && (t->warps_per_tile == 1 || t->warps_per_tile == 2) &&
+			(t->tile_width == 16 || t->tile_width == 32);
+	if (!ok) {
+		return fail(c, CT_ERR_ARG, "ct_ctx_set_tuning: p2p_stage 64/128/256, warps_per_tile 1/2, tile_width 16/32");
+	}
+	c->tune = *t;
+	return CT_OK;
+}
+
+ct_status ct_ctx_get_tuning(const ct_ctx* ctx, ct_tuning* t) {
+	const Ctx* c = (const Ctx*) ctx;
+	if (!c || !t) {
+		return CT_ERR_ARG;
+	}
+	*t = c->tune;
+	return CT_OK;
+}
+
 ct_status ct_fp32_peak(ct_ctx* ctx, double* tflops) {
 	Ctx* c = (Ctx*) ctx;
 	if (!c || !tflops) {

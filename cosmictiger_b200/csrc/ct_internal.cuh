@@ -156,6 +156,7 @@ struct Ctx {
 	// P2L) run side by side: forked from `stream` by fork_ev and joined back by join_ev
 	cudaStream_t side[2] = { nullptr, nullptr };
 	cudaEvent_t fork_ev = nullptr, join_ev[2] = { nullptr, nullptr };
+	ct_tuning tune = { 128, 1, 32 };  // P2P cell-list size, warps per tile, sinks per tile
 	bool drift_timed = false;         // ev[6], ev[7] hold a recorded drift
 	unsigned long long launches = 0;  // kernels of this library launched so far
 	int compensated = 1;              // Neumaier-compensated P2P batch sums

@@ -725,7 +725,6 @@ __device__ __forceinline__ void ksum(float& s, float& comp, float v) {
 // P2P (a warp per 32-sink tile of a leaf; the particles of its P2P source leaves staged per
 // warp in shared memory as offsets from the leaf centre), then M2P + L2P + kick per tile.
 constexpr int P2P_TPB = 256;
-constexpr int P2P_STAGE = 128;
 
 struct P2PArgs {
 	int nsub;
@@ -744,6 +743,7 @@ struct P2PArgs {
 	double* pairs;
 	double* near_pairs;
 	unsigned long long* next;  // work counter: warps take tiles in list order
+	int tw;                    // sinks per tile (32, or 16: every tile through the SMALL path)
 };
 
 // Approximate reciprocal square root (the MUFU unit), flushing denormals: pair separations
@@ -835,12 +835,14 @@ __device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
 // Staged sources of one warp: positions relative to the sink leaf's centre, x and y of source
 // pairs interleaved (x_2i, x_2i+1, y_2i, y_2i+1) and z by quads, so that a pair of sources
 // arrives as aligned register pairs for the f32x2 instructions.
+template<int STAGE>
 struct P2PStage {
-	float4 xy[P2P_STAGE / 2];
-	float4 z[P2P_STAGE / 4];
+	float4 xy[STAGE / 2];
+	float4 z[STAGE / 4];
 };
 
-__device__ __forceinline__ void stage_put(P2PStage* st, int j, float x, float y, float z) {
+template<int STAGE>
+__device__ __forceinline__ void stage_put(P2PStage<STAGE>* st, int j, float x, float y, float z) {
 	float* xy = reinterpret_cast<float*>(st->xy);
 	xy[4 * (j >> 1) + (j & 1)] = x;
 	xy[4 * (j >> 1) + 2 + (j & 1)] = y;
@@ -848,7 +850,8 @@ __device__ __forceinline__ void stage_put(P2PStage* st, int j, float x, float y,
 }
 
 // One staged source against one sink with the per-pair softening test.
-__device__ __forceinline__ void p2p_checked(const P2PStage* st, int j, float kx, float ky, float kz, float h2, float hinv, float h2inv, float h3inv,
+template<int STAGE>
+__device__ __forceinline__ void p2p_checked(const P2PStage<STAGE>* st, int j, float kx, float ky, float kz, float h2, float hinv, float h2inv, float h3inv,
 		float& fx, float& fy, float& fz, float& pt) {
 	const float* xy = reinterpret_cast<const float*>(st->xy);
 	const float dx = kx - xy[4 * (j >> 1) + (j & 1)];
@@ -869,8 +872,8 @@ __device__ __forceinline__ void p2p_checked(const P2PStage* st, int j, float kx,
 //
 // Sources [jb, je) of the chunk (jb a multiple of 4): the whole chunk for a full tile, a slice
 // for one replica of a small tile.
-template<bool CHECK>
-__device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int jb, int je, float kx, float ky, float kz, float h2, float hinv,
+template<bool CHECK, int STAGE>
+__device__ __forceinline__ void p2p_chunk(const P2PStage<STAGE>* __restrict__ st, int jb, int je, float kx, float ky, float kz, float h2, float hinv,
 		float h2inv, float h3inv, float& fx, float& fy, float& fz, float& pt) {
 	int j = jb;
 	const f2 KX = f2_pack(kx, kx), KY = f2_pack(ky, ky), KZ = f2_pack(kz, kz);
@@ -908,13 +911,13 @@ __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int j
 		az = f2_fma(dz1, r31, az);
 		ap = f2_sub(ap, r11);
 	};
-	if (!CHECK && jb == 0 && je == P2P_STAGE) {
+	if (!CHECK && jb == 0 && je == STAGE) {
 		// a full chunk: constant offsets, no loop arithmetic
 #pragma unroll
-		for (int q = 0; q < P2P_STAGE; q += 4) {
+		for (int q = 0; q < STAGE; q += 4) {
 			quad(q);
 		}
-		j = P2P_STAGE;
+		j = STAGE;
 	} else {
 #pragma unroll 2
 		for (; j + 3 < je; j += 4) {
@@ -935,17 +938,46 @@ __device__ __forceinline__ void p2p_chunk(const P2PStage* __restrict__ st, int j
 	}
 }
 
+// The two warps of pair `pair` (warps 2 pair and 2 pair + 1 of the block) meet here: a named
+// barrier of 64 threads (ids 1.., id 0 being __syncthreads').
+__device__ __forceinline__ void pair_sync(int pair) {
+	asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
+}
+
 // SMALL: tiles of at most 16 sinks.  S' = S rounded up to a power of two lanes hold the sinks
 // (lanes past S repeat a sink and are not written); the 32 / S' groups of S' lanes (replicas)
 // each take a contiguous slice of every staged chunk and are added by a butterfly at the end.
-template<bool SMALL>
+// STAGE: sources staged per chunk (the cell-list size).  WPT: warps per tile; with 2, the
+// warps of a pair take one tile together, each every other chunk of its sources, and the
+// second warp's sums are added to the first's in a fixed order (deterministic).
+template<bool SMALL, int STAGE, int WPT>
 __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
-	__shared__ P2PStage stage[P2P_TPB / 32];
+	static_assert(WPT == 1 || WPT == 2, "one or two warps per tile");
+	__shared__ P2PStage<STAGE> stage[P2P_TPB / 32];
+	__shared__ float4 comb[WPT > 1 ? P2P_TPB / 64 : 1][2][32];
+	__shared__ long long pair_tile[P2P_TPB / 64];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-	P2PStage* my = &stage[w];
+	const int pw = WPT > 1 ? (w & 1) : 0, pair = w >> 1;
+	P2PStage<STAGE>* my = &stage[w];
 	double npairs = 0.0, nnear = 0.0;
-	// a resident grid; each warp takes the next tile when it is done with one
-	for (int64_t it = warp_take(a.next, 1); it < a.nitems; it = warp_take(a.next, 1)) {
+	// a resident grid; each warp (pair of warps) takes the next tile when it is done with one
+	for (;;) {
+		int64_t it;
+		if (WPT == 1) {
+			it = warp_take(a.next, 1);
+		} else {
+			if (pw == 0) {
+				const int64_t t = warp_take(a.next, 1);
+				if (lane == 0) {
+					pair_tile[pair] = t;
+				}
+			}
+			pair_sync(pair);
+			it = pair_tile[pair];
+		}
+		if (it >= a.nitems) {
+			break;
+		}
 		const int2 item = a.items[it];
 		const NodeW self = a.nodes[item.x];
 		const float h = a.sub_h ? a.sub_h[box_of(a.sub_off, a.nsub, self.pbeg)] : a.h;
@@ -955,13 +987,13 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 		const float near2 = h2 * 1.01f;
 		int sl = lane, rep = 0, Sp = 32;
 		if (SMALL) {
-			const int S = max(1, self.pend - (self.pbeg + 32 * item.y));  // 1..16
+			const int S = max(1, min(a.tw, self.pend - (self.pbeg + a.tw * item.y)));  // 1..16
 			Sp = S <= 1 ? 1 : 1 << (32 - __clz(S - 1));
 			sl = lane & (Sp - 1);
 			rep = lane / Sp;
 			sl = sl < S ? sl : sl - S;  // sl < Sp < 2S
 		}
-		const int k = self.pbeg + 32 * item.y + sl;
+		const int k = self.pbeg + a.tw * item.y + sl;
 		const bool active = SMALL ? (rep == 0 && (lane & (Sp - 1)) == sl) : k < self.pend;
 		float kx = 0.f, ky = 0.f, kz = 0.f;
 		if (SMALL || active) {
@@ -985,7 +1017,7 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 				near = box_gap2(a.nbox + 6 * (int64_t) item.x, a.nbox + 6 * (int64_t) sl) <= near2;
 			}
 			// far leaves first, then near ones; the particles of one class form a single flat
-			// sequence (prefix sums of the leaf sizes over lanes), staged P2P_STAGE at a time
+			// sequence (prefix sums of the leaf sizes over lanes), staged STAGE at a time
 			for (int cls = 0; cls < 2; cls++) {
 				const bool check = cls != 0;
 				const int c = near == check ? cnt : 0;
@@ -997,10 +1029,10 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 				}
 				const int total = __shfl_sync(0xffffffffu, inc, 31);
 				const int first = beg - (inc - c);  // particle index = first[owner] + flat index
-				for (int gb = 0; gb < total; gb += P2P_STAGE) {
-					const int n = min(P2P_STAGE, total - gb);
+				for (int gb = (WPT > 1 ? pw * STAGE : 0); gb < total; gb += WPT * STAGE) {
+					const int n = min(STAGE, total - gb);
 #pragma unroll
-					for (int j = lane; j < P2P_STAGE; j += 32) {
+					for (int j = lane; j < STAGE; j += 32) {
 						const int g = gb + j;
 						// owner lane of flat index g: the lanes whose inclusive prefix is <= g
 						int l = 0;
@@ -1023,9 +1055,9 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 						je = min(n, jb + sub);
 					}
 					if (check) {
-						p2p_chunk<true>(my, jb, je, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+						p2p_chunk<true, STAGE>(my, jb, je, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 					} else {
-						p2p_chunk<false>(my, jb, je, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
+						p2p_chunk<false, STAGE>(my, jb, je, kx, ky, kz, h2, hinv, h2inv, h3inv, fx, fy, fz, pt);
 					}
 					__syncwarp();
 					if (a.compensated) {
@@ -1045,6 +1077,20 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 			}
 		}
 		float tx = sx + cx, ty = sy + cy, tz = sz + cz, tp = sp + cp;
+		if (WPT > 1) {
+			// the second warp's sums added to the first's (this order in every run)
+			if (pw == 1) {
+				comb[pair][0][lane] = make_float4(tx, ty, tz, tp);
+			}
+			pair_sync(pair);
+			if (pw == 0) {
+				const float4 o = comb[pair][0][lane];
+				tx += o.x;
+				ty += o.y;
+				tz += o.z;
+				tp += o.w;
+			}
+		}
 		if (SMALL) {
 			for (int o = Sp; o < 32; o <<= 1) {
 				tx += __shfl_xor_sync(0xffffffffu, tx, o);
@@ -1054,7 +1100,9 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 			}
 		}
 		if (active) {
-			a.F[k] = make_float4(tx, ty, tz, tp);
+			if (pw == 0) {
+				a.F[k] = make_float4(tx, ty, tz, tp);
+			}
 			npairs += (double) np;
 			nnear += (double) nn;
 		}
@@ -1071,12 +1119,12 @@ __global__ void __launch_bounds__(P2P_TPB, 3) k_p2p(P2PArgs a) {
 
 // Tiles with more than 16 sinks to `big`, the others to `small` (order within each list is
 // immaterial: every tile computes its own sinks).
-__global__ void k_split_tiles(const int2* __restrict__ items, int64_t nitems, const NodeW* __restrict__ nodes, int2* big, int2* small,
+__global__ void k_split_tiles(const int2* __restrict__ items, int64_t nitems, const NodeW* __restrict__ nodes, int tw, int2* big, int2* small,
 		unsigned long long* counts) {
 	for (int64_t it = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; it < nitems; it += (int64_t) gridDim.x * blockDim.x) {
 		const int2 item = items[it];
 		const NodeW nd = nodes[item.x];
-		const int S = nd.pend - (nd.pbeg + 32 * item.y);
+		const int S = min(tw, nd.pend - (nd.pbeg + tw * item.y));
 		if (S > 16) {
 			big[atomicAdd(counts, 1ull)] = item;
 		} else {
@@ -1110,9 +1158,10 @@ struct KickTileArgs {
 	double* sums;
 	int* max_rung;
 	unsigned long long* next;  // work counter (resident grid, tiles taken in list order)
+	int tw;                    // sinks per tile (32 or 16)
 };
 
-// M2P, L2P and the kick for one 32-sink tile per warp (gravity.cu:157-211, kick.cu:53-177).
+// M2P, L2P and the kick for one tile (at most 32 sinks) per warp (gravity.cu:157-211, kick.cu:53-177).
 // Sums of the kick return go to one set per box: block-reduced for a single box, per tile
 // (warp-reduced, atomically added to the tile's box) for an ensemble.
 template<class Ops>
@@ -1136,10 +1185,10 @@ __global__ void __launch_bounds__(128, 3) k_leaf_kick(KickTileArgs a) {
 		const float hinv = 1.f / hh;
 		// S sinks in this tile; with at most 16, R = 32 / S lanes (replicas) share each sink's
 		// M2P list (replica r takes every R-th source node); every lane holds a real sink
-		const int S = max(1, min(32, self.pend - (self.pbeg + 32 * item.y)));
+		const int S = max(1, min(a.tw, self.pend - (self.pbeg + a.tw * item.y)));
 		const int R = S <= 16 ? 32 / S : 1;
 		const int sink = lane % S, rep = lane / S;
-		const int k = self.pbeg + 32 * item.y + sink;
+		const int k = self.pbeg + a.tw * item.y + sink;
 		const bool active = rep == 0;
 		const uint32_t X[3] = { a.x[0][k], a.x[1][k], a.x[2][k] };
 		float Fx = 0.f, Fy = 0.f, Fz = 0.f, Fp = rep == 0 ? (693.f / 256.f) * hinv : 0.f;
@@ -1298,11 +1347,11 @@ __global__ void __launch_bounds__(128, 3) k_leaf_kick(KickTileArgs a) {
 	}
 }
 
-// 32-sink tiles of every leaf: counts, then (leaf, tile) items at the scanned offsets.
-__global__ void k_tile_count(int64_t nleaves, const int64_t* leaves, const NodeW* nodes, int* ntiles) {
+// Tiles of tw sinks of every leaf: counts, then (leaf, tile) items at the scanned offsets.
+__global__ void k_tile_count(int64_t nleaves, const int64_t* leaves, const NodeW* nodes, int tw, int* ntiles) {
 	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nleaves; i += (int64_t) gridDim.x * blockDim.x) {
 		const NodeW nd = nodes[leaves[i]];
-		ntiles[i] = (nd.pend - nd.pbeg + 31) / 32;
+		ntiles[i] = (nd.pend - nd.pbeg + tw - 1) / tw;
 	}
 }
 __global__ void k_tile_fill(int64_t nleaves, const int64_t* leaves, const int* ntiles, const int* off, int2* items) {
@@ -1337,6 +1386,26 @@ int resident_blocks(const Ctx* c, K kernel, int tpb) {
 		nb = 1;
 	}
 	return nb * c->nsm;
+}
+
+// One launch of the P2P kernel instance the context's tuning names (cell-list size, warps per
+// tile): a resident grid, at most one block per 8 tiles.
+template<bool SMALL, int STAGE, int WPT>
+void launch_p2p_t(const Ctx* c, const P2PArgs& pa, int64_t ntiles, cudaStream_t st) {
+	const int64_t want = (ntiles * WPT + 7) / 8;
+	const int nb = (int) std::max<int64_t>(1, std::min<int64_t>(want, (int64_t) resident_blocks(c, k_p2p<SMALL, STAGE, WPT>, P2P_TPB)));
+	k_p2p<SMALL, STAGE, WPT><<<nb, P2P_TPB, 0, st>>>(pa);
+}
+template<bool SMALL>
+void launch_p2p(const Ctx* c, const P2PArgs& pa, int64_t ntiles, cudaStream_t st) {
+	const int s = c->tune.p2p_stage, w = c->tune.warps_per_tile;
+	if (s == 64) {
+		w == 2 ? launch_p2p_t<SMALL, 64, 2>(c, pa, ntiles, st) : launch_p2p_t<SMALL, 64, 1>(c, pa, ntiles, st);
+	} else if (s == 256) {
+		w == 2 ? launch_p2p_t<SMALL, 256, 2>(c, pa, ntiles, st) : launch_p2p_t<SMALL, 256, 1>(c, pa, ntiles, st);
+	} else {
+		w == 2 ? launch_p2p_t<SMALL, 128, 2>(c, pa, ntiles, st) : launch_p2p_t<SMALL, 128, 1>(c, pa, ntiles, st);
+	}
 }
 
 struct KickBuffers {
@@ -1532,7 +1601,9 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			void* tmp = scratch(c, 42, need + 256, &s2);
 			CT_TRY(s2);
 			c->launches++;
-			k_tile_count<<<(int) std::max<int64_t>(1, std::min<int64_t>((nleaves + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nleaves, K.leaves, b->nodes, ntl);
+			const int tw = c->tune.tile_width;
+			k_tile_count<<<(int) std::max<int64_t>(1, std::min<int64_t>((nleaves + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nleaves, K.leaves, b->nodes, tw,
+					ntl);
 			CT_CUDA(c, cudaMemsetAsync(ntl + nleaves, 0, sizeof(int), st));
 			CT_CUDA(c, cub::DeviceScan::ExclusiveSum(tmp, need, ntl, off, (int) nleaves + 1, st));
 			CT_CUDA(c, cudaMemcpyAsync(hf, off + nleaves, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1561,6 +1632,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			pa.compensated = c->compensated;
 			pa.pairs = counters + 4 + 7;
 			pa.near_pairs = counters + 13;
+			pa.tw = tw;
 			// full tiles and tiles of at most 16 sinks go to separate launches
 			int2* tiles2 = (int2*) scratch(c, 45, sizeof(int2) * 2 * (nitems + 1), &s2);
 			CT_TRY(s2);
@@ -1570,8 +1642,8 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			CT_CUDA(c, cudaMemsetAsync(wnext, 0, 2 * sizeof(unsigned long long), st));
 
 			c->launches++;
-			k_split_tiles<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 255) / 256, c->nsm * 8)), 256, 0, st>>>(items, nitems, b->nodes, tiles2,
-					tiles2 + nitems + 1, tcount);
+			k_split_tiles<<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 255) / 256, c->nsm * 8)), 256, 0, st>>>(items, nitems, b->nodes, tw,
+					tiles2, tiles2 + nitems + 1, tcount);
 			CT_CUDA(c, cudaMemcpyAsync(hf, tcount, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
 			CT_CUDA(c, cudaStreamSynchronize(st));
 			const int64_t nbig = (int64_t) ((unsigned long long*) hf)[0], nsmall = (int64_t) ((unsigned long long*) hf)[1];
@@ -1581,16 +1653,14 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 				pa.nitems = nbig;
 				pa.next = wnext;
 				c->launches++;
-				k_p2p<false><<<(int) std::max<int64_t>(1, std::min<int64_t>((nbig + 7) / 8, (int64_t) resident_blocks(c, k_p2p<false>, P2P_TPB))), P2P_TPB, 0,
-						st>>>(pa);
+				launch_p2p<false>(c, pa, nbig, st);
 			}
 			if (nsmall > 0) {
 				pa.items = tiles2 + nitems + 1;
 				pa.nitems = nsmall;
 				pa.next = wnext + 1;
 				c->launches++;
-				k_p2p<true><<<(int) std::max<int64_t>(1, std::min<int64_t>((nsmall + 7) / 8, (int64_t) resident_blocks(c, k_p2p<true>, P2P_TPB))), P2P_TPB, 0,
-						st>>>(pa);
+				launch_p2p<true>(c, pa, nsmall, st);
 			}
 			cudaEventRecord(c->ev[5], st);
 			KickTileArgs ka;
@@ -1624,6 +1694,7 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 			ka.sums = counters + 4;
 			ka.max_rung = c->d_flags + 48;
 			ka.next = (unsigned long long*) (c->d_flags + 62);
+			ka.tw = tw;
 			CT_CUDA(c, cudaMemsetAsync(ka.next, 0, sizeof(unsigned long long), st));
 			c->launches++;
 			k_leaf_kick<Ops><<<(int) std::max<int64_t>(1, std::min<int64_t>((nitems + 3) / 4, (int64_t) resident_blocks(c, k_leaf_kick<Ops>, 128))), 128, 0,

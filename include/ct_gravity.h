@@ -316,6 +316,24 @@ void* ct_stream(ct_ctx* ctx);
  * studies; the reference adds plainly, gravity.cu:331-343). */
 ct_status ct_ctx_set_compensated(ct_ctx* ctx, int compensated);
 
+/* Launch shape of the particle-particle and leaf-kick kernels, the knobs of the autotuner
+ * (cosmictiger_b200/autotune.py).  The reference fixes them at build time: its P2P stages at
+ * most KICK_PP_MAX = 928 source particles per pass (cosmictiger/kick.hpp:48), its M2P at most
+ * KICK_C_MAX = 32 multipoles (kick.hpp:27), one warp per work item (src/kick.cu:179).
+ *   p2p_stage       source particles staged per pass (the cell-list size): 64, 128 or 256
+ *   warps_per_tile  warps sharing one sink tile's sources: 1 or 2
+ *   tile_width      sinks per tile, for P2P and the leaf kick: 32, or 16 (every tile then
+ *                   spreads each sink's sources / multipoles over two or more lanes)
+ * Results differ from one shape to another only in the order of the per-sink sums (within
+ * float rounding); each shape is deterministic.  Default {128, 1, 32}; others: CT_ERR_ARG. */
+typedef struct {
+	int p2p_stage;
+	int warps_per_tile;
+	int tile_width;
+} ct_tuning;
+ct_status ct_ctx_set_tuning(ct_ctx* ctx, const ct_tuning* tuning);
+ct_status ct_ctx_get_tuning(const ct_ctx* ctx, ct_tuning* tuning);
+
 /* ---- allocation-free variant (no counterpart in the reference)
  *
  * For callers that cannot allocate device memory when they partition rungs: a host driver

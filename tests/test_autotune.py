@@ -93,3 +93,57 @@ def test_rejects_untimed_settings():
     with pytest.raises(ValueError):
         autotune.tune_bucket(ctx, _state(500), candidates=())
     assert not ctx.boxes
+
+
+SHAPE_TIME = {(64, 1, 32): 9.0, (128, 1, 32): 8.0, (256, 1, 32): 7.5, (128, 2, 32): 6.0, (128, 1, 16): 5.0, (256, 2, 16): 7.0}
+SHAPE_ERR = {(128, 1, 16): 3e-5}  # a shape whose forces leave the tolerance (it must not win)
+
+
+class ShapeCtx:
+    def __init__(self):
+        self.shape = (128, 1, 32)
+        self.set_calls = []
+
+    def set_tuning(self, p2p_stage=128, warps_per_tile=1, tile_width=32):
+        self.shape = (p2p_stage, warps_per_tile, tile_width)
+        self.set_calls.append(self.shape)
+
+    def box(self, n):
+        return ShapeBox(self, n)
+
+
+class ShapeBox(FakeBox):
+    def counters(self):
+        t = SHAPE_TIME[self.ctx.shape] * TIME[self.bucket] / 7.0 / len(autotune.PHASES)
+        return {p: t for p in autotune.PHASES}
+
+    def download(self, forces=False):
+        assert forces and self.save
+        rng = np.random.default_rng(self.uploads)
+        perm = rng.permutation(self.n)
+        x, y, z = (a[perm] for a in self.state)
+        g = (x.astype(np.float64) + 2.0 * y + 3.0 * z) * (1.0 + SHAPE_ERR.get(self.ctx.shape, 0.0) + ERR[self.bucket])
+        return {"x": x, "y": y, "z": z, "gx": g, "gy": g, "gz": g}
+
+    def close(self):
+        pass
+
+
+def test_tune_picks_the_fastest_shape_within_the_force_tolerance():
+    ctx = ShapeCtx()
+    n = 500
+    rng = np.random.default_rng(3)
+    state = [rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32) for _ in range(3)] + [np.zeros((n, 3), np.float32), np.zeros(n, np.int8)]
+    res = autotune.tune(ctx, state, h=1e-3, shapes=list(SHAPE_TIME), max_force_rms=1e-5)
+    # the reference runs first and the winner is left set on the context
+    assert ctx.set_calls[0] == (128, 1, 32)
+    assert res["reference"]["p2p_stage"] == 128 and res["reference"]["force_rms"] == 0.0
+    best = (res["best"]["p2p_stage"], res["best"]["warps_per_tile"], res["best"]["tile_width"])
+    assert best == (128, 2, 32), best  # (128, 1, 16) is faster but its forces moved 3e-5
+    assert ctx.shape == best
+    assert len(res["rows"]) == len(SHAPE_TIME)
+    # joint search with leaf sizes, no force limit: the fastest pair overall
+    ctx2 = ShapeCtx()
+    res2 = autotune.tune(ctx2, state, h=1e-3, buckets=(96, 128, 160), shapes=list(SHAPE_TIME), max_force_rms=None)
+    assert (res2["best"]["bucket"], res2["best"]["p2p_stage"], res2["best"]["warps_per_tile"], res2["best"]["tile_width"]) == (160, 128, 1, 16)
+    assert len(res2["rows"]) == 3 * len(SHAPE_TIME)
