@@ -105,6 +105,10 @@ def tune(ctx, state, theta=0.55, h=None, buckets=(128,), shapes=SHAPES, referenc
     box = box_factory() if box_factory else ctx.box(n)
     rows = []
     ref = None
+    # the tree order depends on the leaf size only: particles are matched by position once per
+    # leaf size (a sort of all particles), and the launch shapes of one leaf size compare in
+    # tree order
+    order_of = {}
     try:
         for bucket, shape in cands:
             ctx.set_tuning(*shape)
@@ -118,7 +122,14 @@ def tune(ctx, state, theta=0.55, h=None, buckets=(128,), shapes=SHAPES, referenc
                 if rep > 0:
                     times.append(sum(c[p] for p in PHASES))
                 if rep == repeats:
-                    g = _by_position(box.download(forces=True))
+                    out = box.download(forces=True)
+                    if bucket not in order_of:
+                        order_of[bucket] = (out["x"].copy(), np.lexsort((out["z"], out["y"], out["x"])))
+                    tree_x, order = order_of[bucket]
+                    if not np.array_equal(out["x"], tree_x):
+                        raise RuntimeError("the tree order changed between launch shapes of one leaf size")
+                    g = np.stack([out["gx"][order], out["gy"][order], out["gz"][order]], axis=1).astype(np.float64)
+                    del out
             if ref is None:
                 ref = g
             rows.append({"bucket": bucket, "p2p_stage": shape[0], "warps_per_tile": shape[1], "tile_width": shape[2], "ms": float(min(times)),

@@ -118,8 +118,9 @@ class ShapeBox(FakeBox):
         return {p: t for p in autotune.PHASES}
 
     def download(self, forces=False):
+        # the tree order depends on the leaf size (the bucket), not on the launch shape
         assert forces and self.save
-        rng = np.random.default_rng(self.uploads)
+        rng = np.random.default_rng(self.bucket)
         perm = rng.permutation(self.n)
         x, y, z = (a[perm] for a in self.state)
         g = (x.astype(np.float64) + 2.0 * y + 3.0 * z) * (1.0 + SHAPE_ERR.get(self.ctx.shape, 0.0) + ERR[self.bucket])
