@@ -545,42 +545,59 @@ def _errors(gt, gd):
             "p99_per_particle": float(np.percentile(err, 99)), "mag_p50": float(np.percentile(mag, 50)), "mag_p99": float(np.percentile(mag, 99))}
 
 
-def _pos_key(x, y, z):
-    return (x.astype(np.uint64) << np.uint64(32)) | y.astype(np.uint64), z
+SINK_MARK = 1000.0
+
+
+def mark_sinks(v, sel):
+    """A copy of the velocities with the chosen sinks' x velocity set to -(1000 + k): a kick
+    without its half steps (ascending and descending off) leaves velocities as they are, so the
+    sinks can be found again in any tree order by one scan (find_sinks) instead of a sort."""
+    vm = np.array(v, np.float32, copy=True)
+    vm[sel, 0] = -(SINK_MARK + np.arange(len(sel), dtype=np.float32))
+    return vm
+
+
+def find_sinks(out, nsink):
+    """Rows of the marked sinks in a downloaded state, in the order they were marked."""
+    vx = out["v"][:, 0]
+    rows = np.nonzero(vx <= -SINK_MARK)[0]
+    k = np.rint(-vx[rows] - SINK_MARK).astype(np.int64)
+    if len(rows) != nsink or not np.array_equal(np.sort(k), np.arange(nsink)):
+        raise RuntimeError("marked sinks lost (%d of %d found)" % (len(rows), nsink))
+    idx = np.empty(nsink, np.int64)
+    idx[k] = rows
+    return idx
 
 
 def accuracy(box, nsink, h, N, theta, gate_thetas=(0.5, 0.45, 0.4, 0.35), steps_fn=None):
     """Force error of the kick vs the FP64 direct Ewald sum on nsink seeded sinks at the run's
-    theta, and the force-error gate: the same sinks (matched by position; the positions do not
-    move) at smaller theta, each with the particle-steps/s of the all-particles step
+    theta, and the force-error gate: the same sinks (marked, found again in every tree order)
+    at smaller theta, each with the particle-steps/s of the all-particles step
     (steps_fn(theta) -> ms), until one passes 1e-3 per-particle RMS."""
     import cosmictiger_b200 as ct
 
     rng = np.random.default_rng(4321 + 42)
     base = box.download()  # every kick below starts from these positions (timing steps move them)
+    sel = np.sort(rng.choice(N, size=min(nsink, N), replace=False))
+    vm = mark_sinks(base["v"], sel)
 
     def kick_at(th):
-        box.upload(base["x"], base["y"], base["z"], base["v"], base["rung"])
+        box.upload(base["x"], base["y"], base["z"], vm, base["rung"])
         box.sort_by_rung(0)
         box.tree_create(th, h, 128)
         box.kick(ct.KickParams.make(theta=th, h=h, GM=1.0 / N, eta=0.25 / np.sqrt(693 / 256.0), save_force=True, descending=False, ascending=False))
-        return box.download(forces=True)
+        out = box.download(forces=True)
+        idx = find_sinks(out, len(sel))
+        return np.stack([out["gx"][idx], out["gy"][idx], out["gz"][idx]], 1).astype(np.float64)
 
-    out = kick_at(theta)
-    sel = np.sort(rng.choice(N, size=min(nsink, N), replace=False))
-    sx, sy, sz = out["x"][sel], out["y"][sel], out["z"][sel]
-    dg = box.direct_ewald(sx, sy, sz, h)
+    dg = box.direct_ewald(base["x"][sel], base["y"][sel], base["z"][sel], h)
     gd = np.stack(dg[:3], 1) / N
-    gt = np.stack([out["gx"][sel], out["gy"][sel], out["gz"][sel]], 1).astype(np.float64)
+    gt = kick_at(theta)
     res = {"sinks": int(len(sel)), **_errors(gt, gd),
            "definition": "vs FP64 direct Ewald on seeded sinks: rms = sqrt(sum|dg|^2 / sum|g|^2) (the global norm, dominated by the largest "
                          "forces); per_particle = |dg|/|g| per sink, its rms and 99th percentile (every sink weighted alike, as the "
                          "reference's force test reads its sinks one by one, analytic.cpp:78-89); mag = ||g|-|g_ref||/|g_ref| (that test's "
                          "own measure)"}
-    del out
-    # the gate: the sinks' rows in each new tree order, by position
-    k0, z0 = _pos_key(sx, sy, sz)
-    order0 = np.lexsort((z0, k0))
     rows = [{"theta": theta, **{k: res[k] for k in ("rms", "rms_per_particle", "p99_per_particle")}}]
     if steps_fn:
         rows[0]["ms_all_particles_step"] = steps_fn(theta)
@@ -588,16 +605,7 @@ def accuracy(box, nsink, h, N, theta, gate_thetas=(0.5, 0.45, 0.4, 0.35), steps_
     for th in gate_thetas:
         if rows[-1]["rms_per_particle"] <= 1e-3:
             break
-        o = kick_at(th)
-        k, zz = _pos_key(o["x"], o["y"], o["z"])
-        ordr = np.lexsort((zz, k))
-        pos = np.searchsorted(k[ordr], k0[order0])
-        idx = ordr[pos]
-        assert np.array_equal(k[idx], k0[order0]) and np.array_equal(zz[idx], z0[order0])
-        g2 = np.empty_like(gt)
-        g2[order0] = np.stack([o["gx"][idx], o["gy"][idx], o["gz"][idx]], 1)
-        del o
-        e = _errors(g2, gd)
+        e = _errors(kick_at(th), gd)
         row = {"theta": th, **{q: e[q] for q in ("rms", "rms_per_particle", "p99_per_particle")}}
         if steps_fn:
             row["ms_all_particles_step"] = steps_fn(th)
@@ -839,19 +847,22 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def force_errors(box, theta, h, N, nsink, seed):
-    """Kick every particle with save_force, then compare nsink seeded sinks with the FP64
-    direct Ewald sum (same definitions as the benchmark line's force_error)."""
+def force_errors(box, state, theta, h, N, sel, gd):
+    """Kick every particle of `state` (its sinks `sel` marked) with save_force, then compare the
+    sinks with the FP64 direct Ewald forces gd (same definitions as the benchmark line's
+    force_error)."""
     import cosmictiger_b200 as ct
     from cosmictiger_b200 import ics
 
+    x, y, z, v, r = state
+    box.upload(x, y, z, mark_sinks(v, sel), r)
+    box.sort_by_rung(0)
     box.tree_create(theta, h, 128)
     box.kick(ct.KickParams.make(theta=theta, h=h, GM=1.0 / N, eta=ics.eta_default(), save_force=True, descending=False, ascending=False))
     out = box.download(forces=True)
-    sel = np.sort(np.random.default_rng(seed).choice(N, size=min(nsink, N), replace=False))
-    dg = box.direct_ewald(out["x"][sel], out["y"][sel], out["z"][sel], h)
-    gt = np.stack([out["gx"][sel], out["gy"][sel], out["gz"][sel]], 1).astype(np.float64)
-    gd = np.stack(dg[:3], 1) / N
+    idx = find_sinks(out, len(sel))
+    gt = np.stack([out["gx"][idx], out["gy"][idx], out["gz"][idx]], 1).astype(np.float64)
+    del out
     err = np.linalg.norm(gt - gd, axis=1) / np.linalg.norm(gd, axis=1)
     return {"rms": float(np.sqrt(np.sum((gt - gd) ** 2) / np.sum(gd ** 2))), "rms_per_particle": float(np.sqrt(np.mean(err ** 2))),
             "p99_per_particle": float(np.percentile(err, 99))}
@@ -891,18 +902,25 @@ def study_precision(args, torch):
     N = len(state[0])
     h = ics.softening(N, 0.02)
     nsink = args.accuracy_sinks if args.accuracy_sinks > 0 else 1000
+    sel = np.sort(np.random.default_rng(4321).choice(N, size=min(nsink, N), replace=False))
     rows = []
+    gd = None
     for order in (5, 7):
         ctx = ct.Context(order=order)
         lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
         box = ctx.box(N)
+        if gd is None:
+            # the FP64 direct Ewald forces on the sinks, once (positions are the same in every run)
+            box.upload(*state)
+            dg = box.direct_ewald(state[0][sel], state[1][sel], state[2][sel], h)
+            gd = np.stack(dg[:3], 1) / N
         for theta in (0.4, 0.55, 0.7):
             for comp in (True, False):
                 ctx.set_compensated(comp)
                 box.upload(*state)
+                box.sort_by_rung(0)
                 ms = timed_steps(torch, ctx, box, theta, h, N, 2, lib_stream)
-                box.upload(*state)
-                err = force_errors(box, theta, h, N, nsink, seed=4321)
+                err = force_errors(box, state, theta, h, N, sel, gd)
                 row = {"order": order, "theta": theta, "summation": "compensated" if comp else "plain", "ms_per_step": ms,
                        "particle_steps_s": N / (ms / 1e3), **err}
                 rows.append(row)
