@@ -64,6 +64,8 @@ def parse():
                          "(Poisson arrivals of 32^3..256^3 requests, rate sweep, p50/p99 latency vs sequential runs) or lightcone "
                          "(drift with the lightcone capture vs plain drift) or fourier (IC generator and power spectrum on an n^3 grid)")
     ap.add_argument("--study-seed", type=int, default=11)
+    ap.add_argument("--serving-lanes", type=int, default=2, help="serving study: device contexts (streams), each driven by its own host thread")
+    ap.add_argument("--serving-requests", type=int, default=48, help="serving study: requests per arrival rate")
     return ap.parse_args()
 
 
@@ -951,30 +953,34 @@ def study_ensemble(args, torch):
 def study_serving(args, torch):
     """Continuous batching: open-loop Poisson arrivals of requests for boxes of n^3 particles, n
     log-uniform in [32, 256], 1-16 steps each, admission by a 150 GB device-memory budget; a sweep
-    of arrival rates, each against the same requests served one at a time in arrival order."""
+    of arrival rates up to and above saturation, each against the same requests served one at a
+    time in arrival order.  The server runs --serving-lanes lanes (contexts with their own
+    streams, each driven by its own host thread)."""
     import cosmictiger_b200 as ct
     from cosmictiger_b200 import serving
 
-    ctx = ct.Context(order=7)
-    count = 24
+    lanes = [ct.Context(order=7) for _ in range(max(1, args.serving_lanes))]
+    ctx = lanes[0]
+    count = args.serving_requests
     states = {}
     out = []
-    for rate in (1.0, 2.0, 4.0, 8.0):
+    for rate in (1.0, 2.0, 4.0, 8.0, 16.0):
         reqs = serving.poisson_requests(count, rate=rate, nmin=32, nmax=256, smin=1, smax=16, seed=args.study_seed)
         for r in reqs:
             if r.rid not in states:
                 states[r.rid] = serving.request_state(r)
-        srv = serving.Server(ctx, theta=args.theta, hbm_budget=150e9)
+        srv = serving.Server(lanes, theta=args.theta, hbm_budget=150e9)
         done = srv.run(reqs, states)
         s_b = serving.summarize(done)
         seq = serving.poisson_requests(count, rate=rate, nmin=32, nmax=256, smin=1, smax=16, seed=args.study_seed)
         s_p = serving.summarize(serving.run_sequential(ctx, seq, states, theta=args.theta))
-        row = {"rate_per_s": rate, "requests": count, "batched": s_b, "sequential": s_p, "ticks": srv.ticks,
-               "throughput_ratio": s_b["particle_steps_s"] / s_p["particle_steps_s"]}
+        row = {"rate_per_s": rate, "requests": count, "lanes": len(lanes), "batched": s_b, "sequential": s_p, "ticks": srv.ticks,
+               "throughput_ratio": s_b["particle_steps_s"] / s_p["particle_steps_s"], "p99_ratio": s_b["p99_ms"] / s_p["p99_ms"]}
         out.append(row)
         print(json.dumps(row), flush=True)
-    ctx.close()
-    return {"study": "serving", "n_range": [32, 256], "steps_range": [1, 16], "hbm_budget_gb": 150, "rows": out}
+    for c in lanes:
+        c.close()
+    return {"study": "serving", "n_range": [32, 256], "steps_range": [1, 16], "hbm_budget_gb": 150, "lanes": len(lanes), "rows": out}
 
 
 def study_lightcone(args, torch):

@@ -21,6 +21,7 @@
 //                (gravity.cu:157-211,246-404, kick.cu:53-177).
 #include <cub/cub.cuh>
 #include <cstdlib>
+#include <mutex>
 
 #include "ct_internal.cuh"
 #include "ct_ops.cuh"
@@ -1753,32 +1754,43 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 
 }  // namespace
 
-ct_status ewald_init(Ctx* c) {
+// The tables live in __constant__ memory, one copy per device shared by every context on it:
+// they are written once per device and order (the first context created there), so that a
+// context created later never rewrites them while another context's kernels read them, and
+// the host-side index table is built once per process.
+template<class Tab, class Build, class Four>
+ct_status ewald_init_order(Ctx* c, const Tab& sym, int which, Build build, Four four) {
+	static std::mutex m;
+	static bool written[64][2] = {};
+	static Tab h;
+	static std::once_flag h_once;
+	std::call_once(h_once, [&] { build(h); });
+	int dev = 0;
+	CT_CUDA(c, cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(m);
+	if (dev >= 0 && dev < 64 && written[dev][which]) {
+		return CT_OK;
+	}
 	cudaStream_t st = c->stream;
-	if (c->order == 5) {
-		static ct_p5::EwaldTab h;
-		ct_p5::ewald_build_indices(h);
-		ct_p5::EwaldTab* d = nullptr;
-		CT_TRY(dalloc(c, (void**) &d, sizeof(h), "Ewald tables"));
-		CT_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
-		c->launches++;
-		k_ewald_four5<<<1, 128, 0, st>>>(d);
-		CT_CUDA(c, cudaMemcpyToSymbolAsync(c_tab5, d, sizeof(h), 0, cudaMemcpyDeviceToDevice, st));
-		CT_CUDA(c, cudaStreamSynchronize(st));
-		dfree(c, d, sizeof(h));
-	} else {
-		static ct_p7::EwaldTab h;
-		ct_p7::ewald_build_indices(h);
-		ct_p7::EwaldTab* d = nullptr;
-		CT_TRY(dalloc(c, (void**) &d, sizeof(h), "Ewald tables"));
-		CT_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
-		c->launches++;
-		k_ewald_four7<<<1, 128, 0, st>>>(d);
-		CT_CUDA(c, cudaMemcpyToSymbolAsync(c_tab7, d, sizeof(h), 0, cudaMemcpyDeviceToDevice, st));
-		CT_CUDA(c, cudaStreamSynchronize(st));
-		dfree(c, d, sizeof(h));
+	Tab* d = nullptr;
+	CT_TRY(dalloc(c, (void**) &d, sizeof(h), "Ewald tables"));
+	CT_CUDA(c, cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+	c->launches++;
+	four<<<1, 128, 0, st>>>(d);
+	CT_CUDA(c, cudaMemcpyToSymbolAsync(sym, d, sizeof(h), 0, cudaMemcpyDeviceToDevice, st));
+	CT_CUDA(c, cudaStreamSynchronize(st));
+	dfree(c, d, sizeof(h));
+	if (dev >= 0 && dev < 64) {
+		written[dev][which] = true;
 	}
 	return CT_OK;
+}
+
+ct_status ewald_init(Ctx* c) {
+	if (c->order == 5) {
+		return ewald_init_order(c, c_tab5, 0, [](ct_p5::EwaldTab& t) { ct_p5::ewald_build_indices(t); }, k_ewald_four5);
+	}
+	return ewald_init_order(c, c_tab7, 1, [](ct_p7::EwaldTab& t) { ct_p7::ewald_build_indices(t); }, k_ewald_four7);
 }
 
 void kick_buffers_release(Ctx* c) {

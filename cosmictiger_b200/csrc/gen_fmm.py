@@ -283,13 +283,20 @@ def gen_greens(P, accumulate=False):
     return em.text()
 
 
-def gen_radial(P):
-    """Add sum_m n!/(2^m0 m!(n-2m)!) u^(n-2m) g_(N-m0) rinv^m0 into the full tensor Dr (all |n| < P)."""
+def gen_radial(P, stf_from=3):
+    """Add sum_m n!/(2^m0 m!(n-2m)!) u^(n-2m) g_(N-m0) rinv^m0 into the full tensor Dr (all |n| < P).
+
+    For orders N >= stf_from only the m = 0 term u^n g_N is added: every other term carries a
+    Kronecker delta, which the traceless projection of those orders (gen_detrace_full) maps to
+    zero, so the stored tensor after the projection is the same."""
     em = Emitter()
     full = full_set(P)
+    def terms_of(n):
+        return [(0, 0, 0)] if sum(n) >= stf_from else list(half_range(n))
+
     needed = set()
     for n in full:
-        for m in half_range(n):
+        for m in terms_of(n):
             needed.add(sub(n, add(m, m)))
     mon = monomials(em, "u", "ux", "uy", "uz", needed)
     em("const T ri1 = rinv;")
@@ -298,7 +305,7 @@ def gen_radial(P):
     pw = {}
     for n in full:
         N = sum(n)
-        for m in half_range(n):
+        for m in terms_of(n):
             m0 = sum(m)
             pw[(N - m0, m0)] = True
     for (l, m0) in sorted(pw):
@@ -309,7 +316,7 @@ def gen_radial(P):
     for n in full:
         N = sum(n)
         terms = []
-        for m in half_range(n):
+        for m in terms_of(n):
             m0 = sum(m)
             c = Fr(vfact(n), (2 ** m0) * vfact(m) * vfact(sub(n, add(m, m))))
             terms.append((c, (mon[sub(n, add(m, m))], "G%d_%d" % (N - m0, m0))))
@@ -507,7 +514,9 @@ def gen_header(P):
     h.append("}")
     h.append("")
     h.append("// Add the radial-function derivative tensor: Dr[n] += sum_m n!/(2^|m| m!(n-2m)!) u^(n-2m) g_(|n|-|m|) rinv^|m|,")
-    h.append("// where g_k = r^k (r^-1 d/dr)^k f and u the unit vector (full packed symmetric storage).")
+    h.append("// where g_k = r^k (r^-1 d/dr)^k f and u the unit vector (full packed symmetric storage).  Orders >= 3")
+    h.append("// keep only the m = 0 term u^n g_|n|: the others carry a Kronecker delta, which detrace_full's")
+    h.append("// traceless projection of those orders maps to zero, so only the projected sum is meaningful there.")
     h.append("template<class T> CT_HD void radial_add(T* __restrict__ Dr, T ux, T uy, T uz, T rinv, const T* g) {")
     gl = ["\tconst T g%d = g[%d];" % (k, k) for k in range(P)]
     h.extend(gl)

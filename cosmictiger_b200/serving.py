@@ -3,16 +3,20 @@
 A request asks for `steps` gravity steps (tree build + kick + drift, all particles active) of
 its own periodic box of n^3 particles.  The server keeps every admitted request's particles
 resident on the device between steps, admits waiting requests while the device-memory
-budget allows, and advances all active requests together: each tick gathers the active boxes
-into one ensemble (one set of kernel launches for all of them, ct_ensemble_*), runs one step,
-and retires requests whose steps are done.  Requests that arrive while a tick runs join at
-the next tick.  Results do not depend on the mix: boxes of an ensemble never interact and
-every kernel treats them independently, so a request's result is bit-identical alone and
-batched with others.
+budget allows, and advances the active requests in ticks: each tick of a lane gathers its
+small boxes into one ensemble (one set of kernel launches for all of them, ct_ensemble_*),
+steps its large boxes on their own, and retires requests whose steps are done.  Several lanes
+(device contexts with their own streams, each driven by its own host thread) run their ticks
+independently, so that one lane's uploads, host round trips and kernel tails overlap another
+lane's kernels.  Requests that arrive while a tick runs join at a later tick.  Results do not
+depend on the mix: boxes of an ensemble never interact, every kernel treats them
+independently and contexts share no device state that a step writes, so a request's result
+is bit-identical alone and batched with others.
 
 The reference has no serving layer; this one admits requests by a device-memory budget,
 keeps their state resident on the device between steps and reports p50/p99 latency.
 """
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -53,112 +57,151 @@ def request_state(req):
     return ics.zeldovich_lattice(req.n, index=req.index, rms_spacing=req.rms, seed=req.seed)
 
 
-class Server:
-    """Continuous batching.  Requests of at most `plain_above` particles advance together as one
-    ensemble per tick; larger ones advance as their own boxes in the same tick (batching gains
-    little for them and would cost a re-batch whenever membership changes)."""
+class _Lane:
+    """One device context driven by its own host thread: its active requests and its ensemble."""
 
-    def __init__(self, ctx, theta=0.55, hbm_budget=150e9, t0=1.0 / 64, bucket=128, plain_above=1 << 20):
+    def __init__(self, ctx):
         self.ctx = ctx
-        self.plain_above = plain_above
-        self.theta = theta
-        self.budget = hbm_budget
-        self.t0 = t0
-        self.bucket = bucket
-        self.active = []      # [(request, box, remaining steps)]
-        self.waiting = []
-        self.finished = []
+        self.active = []      # [[request, box, remaining steps]]
         self.ens = None
         self.ens_members = None
         self.ens_boxes = []
         self.ens_dirty = False  # the ensemble holds state newer than its member boxes
+        self.hmax = 0.0
         self.ticks = 0
+
+
+class Server:
+    """Continuous batching over one or more lanes.  A lane is a device context (its own CUDA
+    stream) driven by its own host thread; the library releases the interpreter lock while it
+    works, so the lanes' uploads, kernels and host round trips overlap on the device.  Within a
+    lane, requests of at most `plain_above` particles advance together as one ensemble per
+    tick and larger ones advance as their own boxes in the same tick (batching gains little for
+    them and would cost a re-batch whenever membership changes).  A lane holds at most
+    `big_per_lane` large requests at a time, so that large requests start in arrival order
+    across the lanes (first come, first served, as many at once as there are lanes) while
+    small ones join whichever lane takes them first.  Admission keeps the resident particles of
+    all lanes within `hbm_budget` (a request is admitted regardless when nothing is resident)."""
+
+    def __init__(self, ctx, theta=0.55, hbm_budget=150e9, t0=1.0 / 64, bucket=128, plain_above=1 << 20, big_per_lane=1):
+        ctxs = list(ctx) if isinstance(ctx, (list, tuple)) else [ctx]
+        if not ctxs:
+            raise ValueError("a server needs at least one context")
+        if big_per_lane < 1:
+            raise ValueError("big_per_lane must be at least 1")
+        self.lanes = [_Lane(c) for c in ctxs]
+        self.ctx = ctxs[0]
+        self.plain_above = plain_above
+        self.big_per_lane = big_per_lane
+        self.theta = theta
+        self.budget = hbm_budget
+        self.t0 = t0
+        self.bucket = bucket
+        self.waiting = []
+        self.finished = []
+        self.reserved = 0     # device bytes of the requests admitted and not yet retired
+        self.lock = threading.Lock()
         self.particle_steps = 0
+        self.error = None
+
+    @property
+    def ticks(self):
+        return sum(lane.ticks for lane in self.lanes)
 
     def _bytes(self, req):
         return req.particles * BYTES_PER_PARTICLE
 
-    def _in_use(self):
-        return sum(self._bytes(r) for r, _, _ in self.active)
+    def _big(self, req):
+        return req.particles > self.plain_above
 
-    def admit(self, now, states):
-        """Admit waiting requests in arrival order while the budget allows."""
-        keep = []
-        for req in self.waiting:
-            if self._in_use() + self._bytes(req) <= self.budget or not self.active:
-                box = self.ctx.box(req.particles)
-                box.upload(*states[req.rid])
-                req.admitted = now
-                self.active.append([req, box, req.steps])
-            else:
-                keep.append(req)
-        self.waiting = keep
+    def _take(self, lane):
+        """Under the lock: the waiting requests this lane admits now, in arrival order."""
+        big = sum(1 for it in lane.active if self._big(it[0]))
+        take = []
+        for req in list(self.waiting):
+            if self._big(req) and big >= self.big_per_lane:
+                continue
+            if self.reserved + self._bytes(req) <= self.budget or self.reserved == 0:
+                self.reserved += self._bytes(req)
+                self.waiting.remove(req)
+                take.append(req)
+                big += self._big(req)
+        return take
 
-    def _batched(self, item):
-        return item[0].particles <= self.plain_above
+    def _admit(self, lane, reqs, now, states):
+        for req in reqs:
+            box = lane.ctx.box(req.particles)
+            box.upload(*states[req.rid])
+            req.admitted = now
+            lane.active.append([req, box, req.steps])
 
-    def _ensemble(self, batched):
+    def _ensemble(self, lane, batched):
         members = [r.rid for r, _, _ in batched]
-        if members != self.ens_members:
+        if members != lane.ens_members:
             counts = [r.particles for r, _, _ in batched]
-            if self.ens is None:
-                self.ens = self.ctx.ensemble(counts)
+            if lane.ens is None:
+                lane.ens = lane.ctx.ensemble(counts)
             else:
-                if self.ens_dirty:
+                if lane.ens_dirty:
                     # members still running keep their advanced state across the re-batch
-                    self.ens.scatter(self.ens_boxes)
-                # one ensemble for the whole run, re-batched in place (device arrays reused)
-                self.ens.reshape(counts)
+                    lane.ens.scatter(lane.ens_boxes)
+                # one ensemble per lane for the whole run, re-batched in place (device arrays reused)
+                lane.ens.reshape(counts)
             h = np.array([ics.softening(c, 0.02) for c in counts], np.float32)
             gm = np.array([1.0 / c for c in counts], np.float32)
-            self.ens.set_box_params(h, gm)
-            self.ens_boxes = [b for _, b, _ in batched]
-            self.ens.gather(self.ens_boxes)
-            self.ens_dirty = False
-            self.ens_members = members
-            self.hmax = float(h.max())
-        return self.ens
+            lane.ens.set_box_params(h, gm)
+            lane.ens_boxes = [b for _, b, _ in batched]
+            lane.ens.gather(lane.ens_boxes)
+            lane.ens_dirty = False
+            lane.ens_members = members
+            lane.hmax = float(h.max())
+        return lane.ens
 
-    def tick(self, now_fn):
-        """One step of every active request; retire the finished ones."""
-        batched = [it for it in self.active if self._batched(it)]
+    def _tick(self, lane, now_fn):
+        """One step of every active request of the lane; retire the finished ones."""
+        batched = [it for it in lane.active if not self._big(it[0])]
         if batched:
-            ens = self._ensemble(batched)
+            ens = self._ensemble(lane, batched)
             # a request's first step is its run's first call (no ascending half kick)
             ens.set_first_call([int(rem == r.steps) for r, _, rem in batched])
-            ens.tree_create(self.theta, self.hmax, self.bucket)
-            ens.kick(KickParams.make(theta=self.theta, h=self.hmax, GM=1.0, eta=ics.eta_default(), t0=self.t0, first_call=False, save_force=False))
+            ens.tree_create(self.theta, lane.hmax, self.bucket)
+            ens.kick(KickParams.make(theta=self.theta, h=lane.hmax, GM=1.0, eta=ics.eta_default(), t0=self.t0, first_call=False, save_force=False))
             ens.drift(0, 1.0, self.t0)
-            self.ens_dirty = True
-        for req, box, rem in self.active:
-            if req.particles > self.plain_above:
+            lane.ens_dirty = True
+        for req, box, rem in lane.active:
+            if self._big(req):
                 # the plain path, exactly as run_sequential steps a request
                 h = ics.softening(req.particles, 0.02)
                 box.tree_create(self.theta, h, self.bucket)
                 box.kick(KickParams.make(theta=self.theta, h=h, GM=1.0 / req.particles, eta=ics.eta_default(), t0=self.t0, first_call=rem == req.steps,
                                          save_force=False))
                 box.drift(0, 1.0, self.t0)
-        self.ticks += 1
+        lane.ticks += 1
         done = []
-        for item in self.active:
+        stepped = 0
+        for item in lane.active:
             item[2] -= 1
-            self.particle_steps += item[0].particles
+            stepped += item[0].particles
             if item[2] == 0:
                 done.append(item)
         if done:
             # bring the batched boxes' state back, then retire the finished requests
-            if any(self._batched(it) for it in done):
-                self.ens.scatter(self.ens_boxes)
-                self.ens_dirty = False
-                self.ens_members = None  # membership changes
-            self.ctx.synchronize()
+            if any(not self._big(it[0]) for it in done):
+                lane.ens.scatter(lane.ens_boxes)
+                lane.ens_dirty = False
+                lane.ens_members = None  # membership changes
+            lane.ctx.synchronize()
             t = now_fn()
             for item in done:
                 req, box, _ = item
                 req.result = box.download()
                 req.done = t
                 box.close()
-                self.active.remove(item)
+                lane.active.remove(item)
+        with self.lock:
+            self.particle_steps += stepped
+            for req, _, _ in done:
+                self.reserved -= self._bytes(req)
                 self.finished.append(req)
 
     def run(self, requests, states, clock=time.perf_counter):
@@ -166,21 +209,49 @@ class Server:
         pending = sorted(requests, key=lambda r: r.arrival)
         t_start = clock()
         now = lambda: clock() - t_start  # noqa: E731
-        try:
-            while pending or self.waiting or self.active:
+
+        def lane_loop(lane):
+            while self.error is None:
                 t = now()
-                while pending and pending[0].arrival <= t:
-                    self.waiting.append(pending.pop(0))
-                self.admit(t, states)
-                if self.active:
-                    self.tick(now)
-                elif pending:
-                    time.sleep(max(0.0, min(0.01, pending[0].arrival - now())))
+                with self.lock:
+                    while pending and pending[0].arrival <= t:
+                        self.waiting.append(pending.pop(0))
+                    take = self._take(lane)
+                    if not take and not lane.active and not pending and not self.waiting:
+                        return
+                    next_arrival = pending[0].arrival if pending else None
+                self._admit(lane, take, t, states)
+                if lane.active:
+                    self._tick(lane, now)
+                else:
+                    wait = 0.002 if next_arrival is None else next_arrival - now()
+                    time.sleep(max(0.0, min(0.002, wait)))
+
+        def guarded(lane):
+            try:
+                lane_loop(lane)
+            except BaseException as e:  # noqa: BLE001 - handed to the caller after the join
+                with self.lock:
+                    if self.error is None:
+                        self.error = e
+
+        try:
+            if len(self.lanes) == 1:
+                guarded(self.lanes[0])
+            else:
+                threads = [threading.Thread(target=guarded, args=(lane,), daemon=True) for lane in self.lanes]
+                for th in threads:
+                    th.start()
+                for th in threads:
+                    th.join()
+            if self.error is not None:
+                raise self.error
         finally:
-            # also when a step raises: the ensemble's device arrays go back to the context
-            if self.ens is not None:
-                self.ens.close()
-                self.ens = None
+            # also when a step raises: the ensembles' device arrays go back to their contexts
+            for lane in self.lanes:
+                if lane.ens is not None:
+                    lane.ens.close()
+                    lane.ens = None
         return self.finished
 
 

@@ -33,3 +33,27 @@ def test_serving_results_same_alone_and_in_mix(plain_above):
     s = serving.summarize(done)
     assert s["p99_ms"] >= s["p50_ms"] > 0
     ctx.close()
+
+
+def test_serving_two_lanes_results_same_alone_and_in_mix():
+    """Two lanes (two contexts, two host threads, kernels of both on the device at once):
+    every request's result is bit-identical to the request run alone."""
+    import cosmictiger_b200 as ct
+    from cosmictiger_b200 import serving
+
+    lanes = [ct.Context(order=7), ct.Context(order=7)]
+    reqs = serving.poisson_requests(8, rate=400.0, nmin=10, nmax=20, smin=1, smax=4, seed=7)
+    states = {r.rid: serving.request_state(r) for r in reqs}
+    srv = serving.Server(lanes, theta=0.55, hbm_budget=1e12, plain_above=14 ** 3)
+    done = srv.run(reqs, states)
+    assert len(done) == len(reqs)
+    assert all(lane.ticks > 0 for lane in srv.lanes)
+    mixed = {r.rid: r.result for r in done}
+    alone = serving.poisson_requests(8, rate=400.0, nmin=10, nmax=20, smin=1, smax=4, seed=7)
+    for r in alone:
+        r.arrival = 0.0
+        out = serving.run_sequential(lanes[0], [r], states)[0].result
+        for f in ("x", "y", "z", "v", "rung"):
+            assert np.array_equal(out[f], mixed[r.rid][f]), (r.rid, f)
+    for c in lanes:
+        c.close()

@@ -123,3 +123,73 @@ def test_server_plain_path_for_large_requests():
         assert r.result["steps"] == r.steps, (r.rid, r.result, r.steps)
     assert all(ctx.log) and len(ctx.log) == sum(r.steps for r in reqs)
     assert ctx.peak <= sum(r.particles for r in reqs if r.particles <= cut)
+
+
+def test_server_lanes_share_the_work_and_keep_large_requests_in_order():
+    """Two lanes (two contexts, two host threads): every request gets exactly its steps with
+    the right first-call flags, both lanes step requests, no lane ever holds more than one
+    large request, and large requests are admitted in arrival order."""
+    reqs = serving.poisson_requests(60, rate=4000.0, nmin=8, nmax=20, smin=1, smax=9, seed=13)
+    states = {r.rid: () for r in reqs}
+    cut = 12 ** 3
+    lanes = [FakeContext(), FakeContext()]
+    srv = serving.Server(lanes, hbm_budget=1e18, plain_above=cut)
+    big_live = {id(c): 0 for c in lanes}
+    worst = {id(c): 0 for c in lanes}
+    for c in lanes:
+        orig = c.box
+
+        def box(n, c=c, orig=orig):
+            b = orig(n)
+            if n > cut:
+                big_live[id(c)] += 1
+                worst[id(c)] = max(worst[id(c)], big_live[id(c)])
+                close = b.close
+
+                def closing(close=close, c=c):
+                    big_live[id(c)] -= 1
+                    close()
+                b.close = closing
+            return b
+        c.box = box
+    done = srv.run(reqs, states)
+    assert sorted(r.rid for r in done) == list(range(len(reqs)))
+    for r in done:
+        assert r.result["steps"] == r.steps, (r.rid, r.result, r.steps)
+    for c in lanes:
+        assert all(c.log)
+    assert sum(len(c.log) for c in lanes) == sum(r.steps for r in reqs)
+    assert all(lane.ticks > 0 for lane in srv.lanes)
+    assert max(worst.values()) == 1
+    big = sorted((r for r in done if r.particles > cut), key=lambda r: r.arrival)
+    assert [r.admitted for r in big] == sorted(r.admitted for r in big)
+
+
+def test_server_lane_error_reaches_the_caller_and_closes_ensembles():
+    """A step that raises in a lane's thread ends the run with that exception; every lane's
+    ensemble is closed."""
+    reqs = serving.poisson_requests(20, rate=4000.0, nmin=8, nmax=10, smin=2, smax=5, seed=14)
+    states = {r.rid: () for r in reqs}
+    lanes = [FakeContext(), FakeContext()]
+    closed = []
+
+    def failing(c):
+        def ensemble(counts):
+            e = FakeEnsemble(counts, c.log, c.note)
+
+            def kick(params):
+                raise RuntimeError("device step failed")
+            e.kick = kick
+            e.close = lambda: closed.append(1)
+            return e
+        return ensemble
+    for c in lanes:
+        c.ensemble = failing(c)
+    srv = serving.Server(lanes, hbm_budget=1e18)
+    try:
+        srv.run(reqs, states)
+        raise AssertionError("the lane's exception was not raised")
+    except RuntimeError as e:
+        assert "device step failed" in str(e)
+    assert all(lane.ens is None for lane in srv.lanes)
+    assert closed
