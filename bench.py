@@ -135,6 +135,9 @@ def ensemble_compare(ct, torch, ctx, args, theta, lib_stream):
     ctx.synchronize()
     torch.cuda.synchronize()
     ms_b = e0.elapsed_time(e1)
+    cb = ens.counters()
+    breakdown = {k: cb[k] for k in ("ms_tree", "ms_walk", "ms_m2l", "ms_leaf", "ms_leafkick", "cc_ewald", "cc_direct", "cp_pairs", "pp_pairs", "nodes")
+                 if k in cb}
     e0.record(lib_stream)
     for i in range(K):
         plain_step(False)
@@ -151,7 +154,7 @@ def ensemble_compare(ct, torch, ctx, args, theta, lib_stream):
     vp = N * K / (ms_p / 1e3)
     return {"boxes": len(counts), "particles": N, "n_range": [args.ensemble_nmin, args.ensemble_nmax], "steps": K,
             "batched_particle_steps_s": vb, "plain_particle_steps_s": vp, "speedup": vb / vp,
-            "batched_ms_per_step": ms_b / K, "plain_box_ms_p50": float(np.percentile(lat, 50)), "plain_box_ms_p99": float(np.percentile(lat, 99))}
+            "batched_ms_per_step": ms_b / K, "batched_last_kick": breakdown, "plain_box_ms_p50": float(np.percentile(lat, 50)), "plain_box_ms_p99": float(np.percentile(lat, 99))}
 
 
 def make_ics(args, seed):
