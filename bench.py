@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--study-seed", type=int, default=11)
     ap.add_argument("--serving-lanes", type=int, default=2, help="serving study: device contexts (streams), each driven by its own host thread")
     ap.add_argument("--serving-requests", type=int, default=48, help="serving study: requests per arrival rate")
+    ap.add_argument("--serving-big-total", type=int, default=1, help="serving study: large requests (above 2^20 particles) active at once over "
+                    "all lanes (0: one per lane)")
     return ap.parse_args()
 
 
@@ -972,12 +974,12 @@ def study_serving(args, torch):
         for r in reqs:
             if r.rid not in states:
                 states[r.rid] = serving.request_state(r)
-        srv = serving.Server(lanes, theta=args.theta, hbm_budget=150e9)
+        srv = serving.Server(lanes, theta=args.theta, hbm_budget=150e9, big_total=args.serving_big_total or None)
         done = srv.run(reqs, states)
         s_b = serving.summarize(done)
         seq = serving.poisson_requests(count, rate=rate, nmin=32, nmax=256, smin=1, smax=16, seed=args.study_seed)
         s_p = serving.summarize(serving.run_sequential(ctx, seq, states, theta=args.theta))
-        row = {"rate_per_s": rate, "requests": count, "lanes": len(lanes), "batched": s_b, "sequential": s_p, "ticks": srv.ticks,
+        row = {"rate_per_s": rate, "requests": count, "lanes": len(lanes), "big_total": args.serving_big_total or None, "batched": s_b, "sequential": s_p, "ticks": srv.ticks,
                "throughput_ratio": s_b["particle_steps_s"] / s_p["particle_steps_s"], "p99_ratio": s_b["p99_ms"] / s_p["p99_ms"]}
         out.append(row)
         print(json.dumps(row), flush=True)

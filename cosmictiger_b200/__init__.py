@@ -170,6 +170,7 @@ def library():
     L.ct_box_download_device.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.ct_sort_by_rung.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
     L.ct_ctx_set_compensated.argtypes = [vp, i32]
+    L.ct_ctx_set_priority.argtypes = [vp, i32]
     L.ct_ensemble_reshape.argtypes = [vp, i32, i32, ctypes.POINTER(i64)]
     L.ct_box_get_rung_state.argtypes = [vp, i32, ctypes.POINTER(i64), vp, ctypes.POINTER(i32)]
     L.ct_box_set_rung_state.argtypes = [vp, i32, i64, vp, i32]
@@ -254,6 +255,11 @@ class Context:
         t = Tuning()
         self.check(self.lib.ct_ctx_get_tuning(self.h, ctypes.byref(t)), "ct_ctx_get_tuning")
         return {"p2p_stage": t.p2p_stage, "warps_per_tile": t.warps_per_tile, "tile_width": t.tile_width}
+
+    def set_priority(self, priority):
+        """CUDA stream priority of the context (0 default and lowest, negative higher; clamped
+        to the device's range).  Drains the context and replaces its streams."""
+        self.check(self.lib.ct_ctx_set_priority(self.h, int(priority)), "ct_ctx_set_priority")
 
     def set_compensated(self, on):
         """Neumaier-compensated (True, default) or plain FP32 sums of the P2P source batches."""

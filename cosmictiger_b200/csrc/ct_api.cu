@@ -1227,6 +1227,42 @@ ct_status ct_ctx_set_compensated(ct_ctx* ctx, int compensated) {
 	return CT_OK;
 }
 
+ct_status ct_ctx_set_priority(ct_ctx* ctx, int priority) {
+	Ctx* c = (Ctx*) ctx;
+	if (!c) {
+		return CT_ERR_ARG;
+	}
+	cudaSetDevice(c->device);
+	int least = 0, greatest = 0;
+	CT_CUDA(c, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+	const int p = std::min(least, std::max(greatest, priority));  // greatest is the numerically smallest
+	if (p == c->priority) {
+		return CT_OK;
+	}
+	// new streams first (on failure the context keeps its old ones), then drain and swap
+	cudaStream_t ns[3] = { nullptr, nullptr, nullptr };
+	for (int i = 0; i < 3; i++) {
+		if (cudaStreamCreateWithPriority(&ns[i], cudaStreamNonBlocking, p) != cudaSuccess) {
+			for (int k = 0; k < i; k++) {
+				cudaStreamDestroy(ns[k]);
+			}
+			return fail(c, CT_ERR_CUDA, "cudaStreamCreateWithPriority failed");
+		}
+	}
+	cudaStream_t old[3] = { c->stream, c->side[0], c->side[1] };
+	for (int i = 0; i < 3; i++) {
+		cudaStreamSynchronize(old[i]);
+	}
+	c->stream = ns[0];
+	c->side[0] = ns[1];
+	c->side[1] = ns[2];
+	for (int i = 0; i < 3; i++) {
+		cudaStreamDestroy(old[i]);
+	}
+	c->priority = p;
+	return CT_OK;
+}
+
 ct_status ct_ctx_set_tuning(ct_ctx* ctx, const ct_tuning* t) {
 	Ctx* c = (Ctx*) ctx;
 	if (!c || !t) {

@@ -160,6 +160,7 @@ struct Ctx {
 	bool drift_timed = false;         // ev[6], ev[7] hold a recorded drift
 	unsigned long long launches = 0;  // kernels of this library launched so far
 	int compensated = 1;              // Neumaier-compensated P2P batch sums
+	int priority = 0;                 // CUDA stream priority of stream and side[] (0: default)
 	KickBuffers* kick = nullptr;      // owned; grown by the kick, freed with the context
 };
 

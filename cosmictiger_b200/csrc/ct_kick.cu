@@ -428,9 +428,20 @@ __device__ __forceinline__ int64_t warp_take(unsigned long long* next, int chunk
 	}
 	return (int64_t) __shfl_sync(0xffffffffu, v, 0);
 }
+// The node-indexed interaction kernels (Ewald M2L, direct M2L, P2L) visit the nodes of their
+// kind in `order`, longest lists first (nodes without a list of the kind sort last), and each
+// warp of a resident grid takes the next node from `next` when it is done with one: list
+// lengths vary by orders of magnitude, and a static interleave left the busiest SM with
+// 1.2-1.5x the mean SM's work.  Each node's sum is still made by one warp in list order, so
+// the results do not depend on the schedule.
+__device__ __forceinline__ int64_t next_node(unsigned long long* next, const int32_t* __restrict__ order, int64_t nn) {
+	const int64_t k = warp_take(next, 1);
+	return k < nn ? (int64_t) order[k] : -1;
+}
+
 template<class Ops>
-__global__ void __launch_bounds__(128, 3) k_m2l_ewald(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi, const int2* __restrict__ ecc,
-		const int* __restrict__ ecc_list, float* __restrict__ dL, int do_phi, double* counters) {
+__global__ void __launch_bounds__(128, 4) k_m2l_ewald(int64_t nn, const int32_t* __restrict__ order, unsigned long long* next, const NodeW* __restrict__ nodes,
+		const float* __restrict__ multi, const int2* __restrict__ ecc, const int* __restrict__ ecc_list, float* __restrict__ dL, int do_phi, double* counters) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
 	__shared__ float s_real[CT_EWALD_NREAL][3];
 	__shared__ float s_L[4][32][51];
@@ -442,17 +453,14 @@ __global__ void __launch_bounds__(128, 3) k_m2l_ewald(int64_t nn, const NodeW* _
 	const EwaldView<typename Ops::Tab> view { s_real, ct.four, ct.four_exp, ct.D0 };
 	const int lane = threadIdx.x & 31;
 	double icnt_tot = 0;
-	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nw = (gridDim.x * blockDim.x) >> 5;
-	for (int64_t si = gw; si < nn; si += nw) {
+	for (;;) {
+		const int64_t si = next_node(next, order, nn);
+		if (si < 0) {
+			break;
+		}
 		const int2 lst = ecc[si];
 		if (lst.y == 0) {
-			if (lane == 0) {
-				for (int i = 0; i < NE; i++) {
-					dL[NEXP_STRIDE * si + i] = 0.f;
-				}
-			}
-			continue;
+			break;  // the rest of the order holds no Ewald list either (dL is zeroed before the launch)
 		}
 		const NodeW self = nodes[si];
 		// this lane's expansion sum in shared memory (rows of 51 floats: lanes on distinct banks),
@@ -523,15 +531,13 @@ constexpr size_t M2L_DIRECT_SMEM = sizeof(float) * (4 * 32 * 51 + 4 * 2 * 32 * M
 // 32 apart; each lane copies its next source (centre and multipole) into shared memory while
 // it evaluates the current one, so that the gathers from global memory overlap the arithmetic.
 template<class Ops>
-__global__ void __launch_bounds__(128, 3) k_m2l_direct(int64_t nn, const NodeW* __restrict__ nodes, const float* __restrict__ multi,
-		const int2* __restrict__ dcc, const int* __restrict__ dcc_list, float* __restrict__ dL, int do_phi) {
+__global__ void __launch_bounds__(128, 3) k_m2l_direct(int64_t nn, const int32_t* __restrict__ order, unsigned long long* next, const NodeW* __restrict__ nodes,
+		const float* __restrict__ multi, const int2* __restrict__ dcc, const int* __restrict__ dcc_list, float* __restrict__ dL, int do_phi) {
 	constexpr int NE = Ops::NEXP, NM = Ops::NMULT;
 	extern __shared__ __align__(16) float m2l_smem[];
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	float* s_L = m2l_smem;  // [4][32][51]
 	float* my_stage = m2l_smem + 4 * 32 * 51 + ((w * 2) * 32 + lane) * M2L_STAGE;  // stage b at + b * 32 * M2L_STAGE
-	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nw = (gridDim.x * blockDim.x) >> 5;
 	auto stage = [&](int c, int b) {
 		float* d = my_stage + b * 32 * M2L_STAGE;
 		cp_async16(d, nodes + c);
@@ -541,10 +547,14 @@ __global__ void __launch_bounds__(128, 3) k_m2l_direct(int64_t nn, const NodeW* 
 			cp_async16(d + 4 + 4 * k, mp + 4 * k);
 		}
 	};
-	for (int64_t si = gw; si < nn; si += nw) {
+	for (;;) {
+		const int64_t si = next_node(next, order, nn);
+		if (si < 0) {
+			break;
+		}
 		const int2 lst = dcc[si];
 		if (lst.y == 0) {
-			continue;
+			break;  // the rest of the order holds no direct list either
 		}
 		const NodeW self = nodes[si];
 		float* L = s_L + (w * 32 + lane) * 51;
@@ -597,17 +607,20 @@ __global__ void __launch_bounds__(128, 3) k_m2l_direct(int64_t nn, const NodeW* 
 // registers), so lanes stay busy across leaf boundaries; each lane prefetches its next
 // particle's position while it evaluates the current one.
 template<class Ops>
-__global__ void __launch_bounds__(128) k_p2l(int64_t nn, const NodeW* __restrict__ nodes, const int2* __restrict__ cp, const int* __restrict__ cp_list,
-		const uint32_t* __restrict__ x0, const uint32_t* __restrict__ x1, const uint32_t* __restrict__ x2, float* __restrict__ dL, double* counters) {
+__global__ void __launch_bounds__(128, 5) k_p2l(int64_t nn, const int32_t* __restrict__ order, unsigned long long* next, const NodeW* __restrict__ nodes,
+		const int2* __restrict__ cp, const int* __restrict__ cp_list, const uint32_t* __restrict__ x0, const uint32_t* __restrict__ x1,
+		const uint32_t* __restrict__ x2, float* __restrict__ dL, double* counters) {
 	constexpr int NE = Ops::NEXP;
 	const int lane = threadIdx.x & 31;
 	double ncp = 0;
-	const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nw = (gridDim.x * blockDim.x) >> 5;
-	for (int64_t si = gw; si < nn; si += nw) {
+	for (;;) {
+		const int64_t si = next_node(next, order, nn);
+		if (si < 0) {
+			break;
+		}
 		const int2 cpl = cp[si];
 		if (cpl.y == 0 || !(nodes[si].flags & 1)) {
-			continue;
+			break;  // the rest of the order holds no P2L list either (only leaves have one)
 		}
 		const NodeW self = nodes[si];
 		float L[NE];
@@ -673,6 +686,22 @@ __global__ void __launch_bounds__(128) k_p2l(int64_t nn, const NodeW* __restrict
 	}
 	if (lane == 0 && ncp > 0) {
 		atomicAdd(counters + 1, ncp);
+	}
+}
+
+// Sort keys of the three node orders: the bit length of the node's list length of each kind (P2L
+// lists count only at leaves), and the node indices to be sorted with them.  Sorting by the bit
+// length (a stable sort) puts the longest lists first and keeps tree order among lists of
+// similar length, so that warps working at the same time read nearby source nodes.
+constexpr int ORDER_KEY_BITS = 6;  // bit lengths 0..32
+__global__ void k_order_keys(int64_t nn, const NodeW* __restrict__ nodes, const int2* __restrict__ ecc, const int2* __restrict__ dcc,
+		const int2* __restrict__ cp, uint32_t* __restrict__ key, int32_t* __restrict__ idx) {
+	for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nn; i += (int64_t) gridDim.x * blockDim.x) {
+		const uint32_t le = (uint32_t) ecc[i].y, ld = (uint32_t) dcc[i].y, lp = (nodes[i].flags & 1) ? (uint32_t) cp[i].y : 0u;
+		key[i] = 32u - __clz(le);
+		key[nn + i] = 32u - __clz(ld);
+		key[2 * nn + i] = 32u - __clz(lp);
+		idx[i] = (int32_t) i;
 	}
 }
 
@@ -1380,9 +1409,9 @@ __global__ void k_collect_leaves(int64_t nn, const NodeW* nodes, int64_t* leaves
 // Blocks of `tpb` threads of `kernel` resident on the whole GPU (its register and shared
 // memory use decide; at least one per SM).
 template<class K>
-int resident_blocks(const Ctx* c, K kernel, int tpb) {
+int resident_blocks(const Ctx* c, K kernel, int tpb, size_t dyn_smem = 0) {
 	int nb = 0;
-	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, tpb, 0) != cudaSuccess || nb < 1) {
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, tpb, dyn_smem) != cudaSuccess || nb < 1) {
 		cudaGetLastError();
 		nb = 1;
 	}
@@ -1548,25 +1577,48 @@ ct_status kick_t(Ctx* c, Box* b, const ct_kick_params* kp, ct_kick_return* out) 
 		}
 		// ---- interactions
 		CT_CUDA(c, cudaMemsetAsync(counters, 0, 16 * sizeof(double), st));
-		// node-indexed kernels: a static interleave over all nodes (most hold no list of the
-		// kind; a work counter costs more here than the last wave's tail)
-		// The three kernels run side by side on three streams, each into its own expansion
-		// deltas; L2L adds them in this order, dL + dL2 + dL3, the order of one stream.
-		const int gm = c->nsm * 8;
+		// node orders of the three node-indexed kernels, longest lists first (radix sort of the
+		// list lengths' bit lengths; nodes without a list of a kind sort last)
+		ct_status s3 = CT_OK;
+		uint32_t* okey = (uint32_t*) scratch(c, 46, sizeof(uint32_t) * 6 * nn, &s3);
+		int32_t* oidx = (int32_t*) scratch(c, 47, sizeof(int32_t) * 4 * nn, &s3);
+		unsigned long long* onext = (unsigned long long*) scratch(c, 48, 3 * sizeof(unsigned long long), &s3);
+		CT_TRY(s3);
+		size_t sort_bytes = 0;
+		CT_CUDA(c, cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_bytes, okey, okey + 3 * nn, oidx, oidx + nn, (int) nn, 0, ORDER_KEY_BITS, st));
+		void* sort_tmp = scratch(c, 49, sort_bytes + 256, &s3);
+		CT_TRY(s3);
+		c->launches++;
+		k_order_keys<<<(int) std::max<int64_t>(1, std::min<int64_t>((nn + 255) / 256, c->nsm * 8)), 256, 0, st>>>(nn, b->nodes, o.ecc, o.dcc, o.cp, okey,
+				oidx);
+		for (int k = 0; k < 3; k++) {
+			size_t tb = sort_bytes;
+			CT_CUDA(c, cub::DeviceRadixSort::SortPairsDescending(sort_tmp, tb, okey + k * nn, okey + (3 + k) * nn, oidx, oidx + (1 + k) * nn, (int) nn, 0,
+					ORDER_KEY_BITS, st));
+		}
+		CT_CUDA(c, cudaMemsetAsync(onext, 0, 3 * sizeof(unsigned long long), st));
 		const size_t dl_bytes = sizeof(float) * NEXP_STRIDE * nn;
+		CT_CUDA(c, cudaMemsetAsync(K.dL, 0, dl_bytes, st));
+		// The three kernels run side by side on three streams, each into its own expansion
+		// deltas; L2L adds them in this order, dL + dL2 + dL3, the order of one stream.  Each is
+		// a resident grid (blocks per SM from the occupancy query) whose warps take nodes from
+		// the kind's order.
 		CT_CUDA(c, cudaEventRecord(c->fork_ev, st));
 		for (int k = 0; k < 2; k++) {
 			CT_CUDA(c, cudaStreamWaitEvent(c->side[k], c->fork_ev, 0));
 		}
 		c->launches++;
-		k_m2l_ewald<Ops><<<gm, 128, 0, st>>>(nn, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL, kp->do_phi, counters);
+		k_m2l_ewald<Ops><<<resident_blocks(c, k_m2l_ewald<Ops>, 128), 128, 0, st>>>(nn, oidx + nn, onext, b->nodes, b->multi, o.ecc, o.ecc_list, K.dL,
+				kp->do_phi, counters);
 		CT_CUDA(c, cudaMemsetAsync(K.dL2, 0, dl_bytes, c->side[0]));
 		c->launches++;
 		CT_CUDA(c, cudaFuncSetAttribute(k_m2l_direct<Ops>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) M2L_DIRECT_SMEM));
-		k_m2l_direct<Ops><<<gm, 128, M2L_DIRECT_SMEM, c->side[0]>>>(nn, b->nodes, b->multi, o.dcc, o.dcc_list, K.dL2, kp->do_phi);
+		k_m2l_direct<Ops><<<resident_blocks(c, k_m2l_direct<Ops>, 128, M2L_DIRECT_SMEM), 128, M2L_DIRECT_SMEM, c->side[0]>>>(nn, oidx + 2 * nn, onext + 1,
+				b->nodes, b->multi, o.dcc, o.dcc_list, K.dL2, kp->do_phi);
 		CT_CUDA(c, cudaMemsetAsync(K.dL3, 0, dl_bytes, c->side[1]));
 		c->launches++;
-		k_p2l<Ops><<<gm, 128, 0, c->side[1]>>>(nn, b->nodes, o.cp, o.cp_list, b->x[0], b->x[1], b->x[2], K.dL3, counters);
+		k_p2l<Ops><<<resident_blocks(c, k_p2l<Ops>, 128), 128, 0, c->side[1]>>>(nn, oidx + 3 * nn, onext + 2, b->nodes, o.cp, o.cp_list, b->x[0], b->x[1],
+				b->x[2], K.dL3, counters);
 		for (int k = 0; k < 2; k++) {
 			CT_CUDA(c, cudaEventRecord(c->join_ev[k], c->side[k]));
 			CT_CUDA(c, cudaStreamWaitEvent(st, c->join_ev[k], 0));

@@ -606,7 +606,7 @@ def gen_header(P):
 EWALD_TEMPLATE = r"""
 // Periodic (Ewald) correction to the Green's function, d^n(phi_periodic + 1/r), for a separation
 // (x,y,z) inside the unit cell: the n=0 image with the bare 1/r removed (erf series), the
-// real-space images inside the 2.6-box cutoff (erfc, Abramowitz & Stegun 7.1.26), the Fourier
+// real-space images inside the CT_EWALD_RCUT_G cutoff (erfc, Abramowitz & Stegun 7.1.26), the Fourier
 // sum over 0<|h|^2<=8 and the pi/alpha^2 background term, alpha = 2.
 // Follows ewald_greens_function, cosmictiger/fmm_kernels.hpp:310-1491.
 template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y, T z, const Tab& tab) {
@@ -652,18 +652,20 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 	// them in increasing order.  Each thread then loops over its own images only, so the
 	// threads of a warp (each with its own separation) no longer step through the union of
 	// their image sets; the accumulation order is unchanged.
-	static_assert((CT_EWALD_NREAL + 31) / 32 == 6, "six words of image bits");
-	unsigned int inside[6];
+	// Only the first CT_EWALD_NREAL_G images of the table (those within CT_EWALD_RCUT_G of the
+	// unit cell) can be inside the cutoff.
+	static_assert((CT_EWALD_NREAL_G + 31) / 32 == 4, "four words of image bits");
+	unsigned int inside[4];
 	int nin = 0;
-	for (int wd = 0; wd < 6; wd++) {
+	for (int wd = 0; wd < 4; wd++) {
 		unsigned int m = 0u;
-		for (int b = 0; b < 32 && 32 * wd + b < CT_EWALD_NREAL; b++) {
+		for (int b = 0; b < 32 && 32 * wd + b < CT_EWALD_NREAL_G; b++) {
 			const int i = 32 * wd + b;
 			const T dx = x - T(1000) * T(tab.real[i][0]);
 			const T dy = y - T(1000) * T(tab.real[i][1]);
 			const T dz = z - T(1000) * T(tab.real[i][2]);
 			const T r2 = ct_fma(dx, dx, ct_fma(dy, dy, dz * dz));
-			m |= (unsigned int) (r2 < T(1000 * 1000 * 2.6 * 2.6)) << b;
+			m |= (unsigned int) (r2 < T(1000 * 1000 * CT_EWALD_RCUT_G * CT_EWALD_RCUT_G)) << b;
 		}
 		inside[wd] = m;
 		nin += ct_popc(m);
@@ -698,11 +700,17 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 		}
 	}
 	detrace_full(D, Dr);
-	// Fourier terms accumulate straight into the detraced real-space sum
-	for (int i = 0; i < CT_EWALD_NFOUR; i++) {
+	// Fourier terms accumulate straight into the detraced real-space sum.  The vectors h and -h
+	// add the same term (the order-n derivative tensor changes sign by (-1)^n, the sine with
+	// h, so every entry's product is unchanged): the first half of the table holds one vector
+	// of each pair (ewald_build_indices), taken twice.
+	static_assert(CT_EWALD_NFOUR % 2 == 0, "Fourier vectors come in +h/-h pairs");
+	for (int i = 0; i < CT_EWALD_NFOUR / 2; i++) {
 		const T hdotx = ct_fma(T(tab.four[i][0]), x, ct_fma(T(tab.four[i][1]), y, T(tab.four[i][2]) * z));
 		T sn, cn;
 		ct_sincos_poly(T(6.2831853071795865e-3) * hdotx, &sn, &cn);
+		sn *= T(2);
+		cn *= T(2);
 @FOURIER_ACC@
 	}
 	D[0] += T(7.8539816339744831e-4);
@@ -711,8 +719,8 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 
 // Ewald table storage for this order (lives in __constant__ memory on the device).
 struct EwaldTab {
-	float real[CT_EWALD_NREAL][3];       // real-space image vectors, |n|^2 descending
-	float four[CT_EWALD_NFOUR][3];       // Fourier vectors, |h|^2 descending
+	float real[CT_EWALD_NREAL][3];       // real-space image vectors: the CT_EWALD_NREAL_G within CT_EWALD_RCUT_G of the cell first; |n|^2 descending in each part
+	float four[CT_EWALD_NFOUR][3];       // Fourier vectors: one of each +h/-h pair, then the negatives (|h|^2 descending in each half)
 	float four_exp[CT_EWALD_NFOUR][NEXP];  // detraced derivative tensors of the Fourier terms
 	float D0[NFULL];                     // r -> 0 limit of d^n(erf(alpha r)/r), full storage
 };
@@ -758,7 +766,8 @@ CT_HD_FN double ewald_d0_entry(int c) {
 }
 
 // Image and Fourier vectors, each list ordered by |n|^2 descending (ties in enumeration order)
-// (src/ewald_indices.cu:32-66).
+// (src/ewald_indices.cu:32-66); the image list is then split at CT_EWALD_RCUT_G from the unit
+// cell and the Fourier list into +h and -h halves.
 inline void ewald_build_indices(EwaldTab& tab) {
 	int cnt = 0;
 	for (int i = -4; i <= 4; i++) {
@@ -808,7 +817,56 @@ inline void ewald_build_indices(EwaldTab& tab) {
 		}
 	};
 	sort_desc(tab.real, CT_EWALD_NREAL);
+	// the images within CT_EWALD_RCUT_G of the unit cell first (the only ones the kick's Green's
+	// function can reach), the rest after; |n|^2 descending in each part (a stable partition)
+	{
+		float near_[CT_EWALD_NREAL][3], far_[CT_EWALD_NREAL][3];
+		int nn_ = 0, nf_ = 0;
+		for (int a = 0; a < CT_EWALD_NREAL; a++) {
+			double d2 = 0.0;
+			for (int d = 0; d < 3; d++) {
+				const double c = tab.real[a][d] < 0.f ? -tab.real[a][d] - 0.5 : (tab.real[a][d] > 0.f ? tab.real[a][d] - 0.5 : 0.0);
+				d2 += c * c;
+			}
+			float* dst = d2 < CT_EWALD_RCUT_G * CT_EWALD_RCUT_G ? near_[nn_++] : far_[nf_++];
+			for (int d = 0; d < 3; d++) {
+				dst[d] = tab.real[a][d];
+			}
+		}
+		for (int a = 0; a < nn_; a++) {
+			for (int d = 0; d < 3; d++) {
+				tab.real[a][d] = near_[a][d];
+			}
+		}
+		for (int a = 0; a < nf_; a++) {
+			for (int d = 0; d < 3; d++) {
+				tab.real[nn_ + a][d] = far_[a][d];
+			}
+		}
+	}
 	sort_desc(tab.four, CT_EWALD_NFOUR);
+	// one vector of each +h/-h pair (first nonzero component positive) in the first half, the
+	// negatives in the second, each half still by |h|^2 descending (a stable partition)
+	float pos[CT_EWALD_NFOUR][3], neg[CT_EWALD_NFOUR][3];
+	int np = 0, nn = 0;
+	for (int a = 0; a < CT_EWALD_NFOUR; a++) {
+		const float* v = tab.four[a];
+		const bool first = v[0] > 0.f || (v[0] == 0.f && (v[1] > 0.f || (v[1] == 0.f && v[2] > 0.f)));
+		float* dst = first ? pos[np++] : neg[nn++];
+		dst[0] = v[0];
+		dst[1] = v[1];
+		dst[2] = v[2];
+	}
+	for (int a = 0; a < np; a++) {
+		for (int d = 0; d < 3; d++) {
+			tab.four[a][d] = pos[a][d];
+		}
+	}
+	for (int a = 0; a < nn; a++) {
+		for (int d = 0; d < 3; d++) {
+			tab.four[np + a][d] = neg[a][d];
+		}
+	}
 }
 
 // Complete table build on the host in FP64 (the device build runs ewald_four_entry and

@@ -69,6 +69,8 @@ class _Lane:
         self.ens_dirty = False  # the ensemble holds state newer than its member boxes
         self.hmax = 0.0
         self.ticks = 0
+        self.priority = 0     # CUDA stream priority of the lane's context (0 default)
+        self.big = 0          # large requests admitted to this lane and not yet retired (under the server's lock)
 
 
 class Server:
@@ -80,19 +82,31 @@ class Server:
     them and would cost a re-batch whenever membership changes).  A lane holds at most
     `big_per_lane` large requests at a time, so that large requests start in arrival order
     across the lanes (first come, first served, as many at once as there are lanes) while
-    small ones join whichever lane takes them first.  Admission keeps the resident particles of
-    all lanes within `hbm_budget` (a request is admitted regardless when nothing is resident)."""
+    small ones join whichever lane takes them first; `big_total` caps the large requests active
+    at once over all lanes (1: large requests run one at a time, first come first served, while
+    the other lanes step small requests beside them).  With several lanes, the lane that holds the
+    oldest active request runs its streams at the device's highest priority and the others at
+    the default: the oldest request's kernels take the SMs first and the others fill what it
+    leaves idle (host round trips, kernel tails), so that overlapping requests add throughput
+    without stretching the request that started first.  Admission keeps the resident particles
+    of all lanes within `hbm_budget` (a request is admitted regardless when nothing is
+    resident)."""
 
-    def __init__(self, ctx, theta=0.55, hbm_budget=150e9, t0=1.0 / 64, bucket=128, plain_above=1 << 20, big_per_lane=1):
+    HIGH_PRIORITY = -100  # clamped by the library to the device's highest stream priority
+
+    def __init__(self, ctx, theta=0.55, hbm_budget=150e9, t0=1.0 / 64, bucket=128, plain_above=1 << 20, big_per_lane=1, big_total=None):
         ctxs = list(ctx) if isinstance(ctx, (list, tuple)) else [ctx]
         if not ctxs:
             raise ValueError("a server needs at least one context")
         if big_per_lane < 1:
             raise ValueError("big_per_lane must be at least 1")
+        if big_total is not None and big_total < 1:
+            raise ValueError("big_total must be at least 1")
         self.lanes = [_Lane(c) for c in ctxs]
         self.ctx = ctxs[0]
         self.plain_above = plain_above
         self.big_per_lane = big_per_lane
+        self.big_total = big_total  # large requests active at once over all lanes (None: lanes x big_per_lane)
         self.theta = theta
         self.budget = hbm_budget
         self.t0 = t0
@@ -100,6 +114,7 @@ class Server:
         self.waiting = []
         self.finished = []
         self.reserved = 0     # device bytes of the requests admitted and not yet retired
+        self.big_active = 0   # large requests admitted and not yet retired, all lanes
         self.lock = threading.Lock()
         self.particle_steps = 0
         self.error = None
@@ -116,17 +131,27 @@ class Server:
 
     def _take(self, lane):
         """Under the lock: the waiting requests this lane admits now, in arrival order."""
-        big = sum(1 for it in lane.active if self._big(it[0]))
+        cap_all = self.big_total if self.big_total is not None else len(self.lanes) * self.big_per_lane
         take = []
         for req in list(self.waiting):
-            if self._big(req) and big >= self.big_per_lane:
+            if self._big(req) and (lane.big >= self.big_per_lane or self.big_active >= cap_all):
                 continue
             if self.reserved + self._bytes(req) <= self.budget or self.reserved == 0:
                 self.reserved += self._bytes(req)
                 self.waiting.remove(req)
                 take.append(req)
-                big += self._big(req)
+                if self._big(req):
+                    lane.big += 1
+                    self.big_active += 1
         return take
+
+    def _wanted_priority(self, lane):
+        """Under the lock: the stream priority this lane should run at."""
+        if len(self.lanes) == 1 or not lane.active:
+            return 0
+        # snapshots: another lane's thread may be adding to or retiring from its list
+        oldest = min((it[0].arrival, it[0].rid) for ln in self.lanes for it in list(ln.active))
+        return self.HIGH_PRIORITY if any((it[0].arrival, it[0].rid) == oldest for it in list(lane.active)) else 0
 
     def _admit(self, lane, reqs, now, states):
         for req in reqs:
@@ -202,6 +227,9 @@ class Server:
             self.particle_steps += stepped
             for req, _, _ in done:
                 self.reserved -= self._bytes(req)
+                if self._big(req):
+                    lane.big -= 1
+                    self.big_active -= 1
                 self.finished.append(req)
 
     def run(self, requests, states, clock=time.perf_counter):
@@ -222,6 +250,11 @@ class Server:
                     next_arrival = pending[0].arrival if pending else None
                 self._admit(lane, take, t, states)
                 if lane.active:
+                    with self.lock:
+                        want = self._wanted_priority(lane)
+                    if want != lane.priority:
+                        lane.ctx.set_priority(want)
+                        lane.priority = want
                     self._tick(lane, now)
                 else:
                     wait = 0.002 if next_arrival is None else next_arrival - now()

@@ -316,6 +316,13 @@ void* ct_stream(ct_ctx* ctx);
  * studies; the reference adds plainly, gravity.cu:331-343). */
 ct_status ct_ctx_set_compensated(ct_ctx* ctx, int compensated);
 
+/* Scheduling priority of the context's CUDA streams, in CUDA's convention (0 the default and
+ * lowest; negative values higher; clamped to the device's range).  The context is drained and
+ * its streams are replaced, so a handle from ct_stream taken before the call is stale after it.
+ * The reference has no counterpart (one process per GPU); the serving loop gives the lane that
+ * holds the oldest request the higher priority, so that work started first finishes first. */
+ct_status ct_ctx_set_priority(ct_ctx* ctx, int priority);
+
 /* Launch shape of the particle-particle and leaf-kick kernels, the knobs of the autotuner
  * (cosmictiger_b200/autotune.py).  The reference fixes them at build time: its P2P stages at
  * most KICK_PP_MAX = 928 source particles per pass (cosmictiger/kick.hpp:48), its M2P at most

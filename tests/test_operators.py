@@ -86,8 +86,20 @@ def test_ewald_tables(oracle, order):
     d0 = np.zeros(nfull, np.float32)
     oracle.op("ewald_tables", order, real, four, fexp, d0)
     assert set(map(tuple, real)) == set(map(tuple, g["ewald_real"]))
-    assert np.array_equal((real ** 2).sum(1), (g["ewald_real"] ** 2).sum(1))  # |n|^2 descending
+    # the images within 2.3 box lengths of the unit cell lead the table (the kick's Green's
+    # function reads only those), each part by |n|^2 descending as the reference orders them
+    cell = np.sqrt((np.maximum(np.abs(real) - 0.5, 0.0) ** 2).sum(1))
+    ng = 116
+    assert (cell[:ng] < 2.3).all() and (cell[ng:] >= 2.3).all()
+    for part in (real[:ng], real[ng:]):
+        n2 = (part ** 2).sum(1)
+        assert (np.diff(n2) <= 0).all()
     assert set(map(tuple, four)) == set(map(tuple, g["ewald_four"]))
+    # one vector of each +h/-h pair first (first nonzero component positive), then the negatives
+    half = four[:46]
+    assert set(map(tuple, -half)) == set(map(tuple, four[46:]))
+    first = np.array([v[np.nonzero(v)[0][0]] for v in half])
+    assert (first > 0).all()
     ref = {tuple(g["ewald_four"][i]): g["ewald_four_exp"][i] for i in range(92)}
     for i in range(92):
         assert relmax(fexp[i], ref[tuple(four[i])]) < 1e-6

@@ -90,6 +90,9 @@ class FakeContext:
     def synchronize(self):
         pass
 
+    def set_priority(self, p):
+        self.priority = p
+
 
 def test_server_steps_and_budget():
     reqs = serving.poisson_requests(40, rate=5000.0, nmin=8, nmax=20, smin=1, smax=9, seed=11)
@@ -193,3 +196,65 @@ def test_server_lane_error_reaches_the_caller_and_closes_ensembles():
         assert "device step failed" in str(e)
     assert all(lane.ens is None for lane in srv.lanes)
     assert closed
+
+
+def test_lane_with_the_oldest_request_gets_the_high_priority():
+    """The lane holding the oldest active request (earliest arrival) asks for the high stream
+    priority, every other lane for the default; a single lane never changes priority."""
+    lanes = [FakeContext(), FakeContext(), FakeContext()]
+    srv = serving.Server(lanes, hbm_budget=1e18)
+    reqs = serving.poisson_requests(5, rate=10.0, nmin=8, nmax=10, seed=15)
+    a, b, c = srv.lanes
+    a.active = [[reqs[3], None, 1]]
+    b.active = [[reqs[1], None, 1], [reqs[4], None, 1]]
+    c.active = []
+    assert srv._wanted_priority(b) == serving.Server.HIGH_PRIORITY
+    assert srv._wanted_priority(a) == 0
+    assert srv._wanted_priority(c) == 0
+    b.active = [[reqs[4], None, 1]]
+    assert srv._wanted_priority(a) == serving.Server.HIGH_PRIORITY
+    one = serving.Server(FakeContext(), hbm_budget=1e18)
+    one.lanes[0].active = [[reqs[0], None, 1]]
+    assert one._wanted_priority(one.lanes[0]) == 0
+
+
+def test_big_total_runs_large_requests_one_at_a_time_in_arrival_order():
+    """big_total=1 over two lanes: never two large requests resident at once, large requests
+    admitted in arrival order, every request stepped exactly its number of times."""
+    import threading
+
+    reqs = serving.poisson_requests(50, rate=4000.0, nmin=8, nmax=20, smin=1, smax=6, seed=16)
+    states = {r.rid: () for r in reqs}
+    cut = 12 ** 3
+    lanes = [FakeContext(), FakeContext()]
+    live = [0]
+    worst = [0]
+    lock = threading.Lock()
+    for c in lanes:
+        orig = c.box
+
+        def box(n, orig=orig):
+            b = orig(n)
+            if n > cut:
+                with lock:
+                    live[0] += 1
+                    worst[0] = max(worst[0], live[0])
+                close = b.close
+
+                def closing(close=close):
+                    with lock:
+                        live[0] -= 1
+                    close()
+                b.close = closing
+            return b
+        c.box = box
+    srv = serving.Server(lanes, hbm_budget=1e18, plain_above=cut, big_total=1)
+    done = srv.run(reqs, states)
+    assert sorted(r.rid for r in done) == list(range(len(reqs)))
+    for r in done:
+        assert r.result["steps"] == r.steps
+    assert worst[0] == 1
+    big = sorted((r for r in done if r.particles > cut), key=lambda r: r.arrival)
+    assert len(big) > 2
+    assert [r.admitted for r in big] == sorted(r.admitted for r in big)
+    assert srv.big_active == 0 and all(lane.big == 0 for lane in srv.lanes)
