@@ -4,6 +4,8 @@ Integer work (tree keys, particle order, node ranges, fixed-point drift, rung pa
 be bit-exact; node geometry (centres, radii, boxes) too, since it decides the opening tests;
 kick forces and potentials within 1e-5 relative RMS.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -157,6 +159,44 @@ def test_tree_bitexact(ctx, oracle, n, theta, bucket, seed):
     m_a, m_b = a["multi"], b["multi"]
     assert np.max(np.abs(m_a - m_b) / (np.abs(m_b) + 1e-6 * np.abs(m_b[:, :1]) + 1e-30)) < 1e-5
     box.close()
+
+
+REF_TREE = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_tree.npz"))
+
+
+@pytest.mark.parametrize("case", sorted({k.split("/")[0] for k in REF_TREE.files}))
+def test_tree_matches_reference_fixtures(ctx, case):
+    """The device tree build against the reference's own tree_create and particles_sort
+    (tests/golden/ref_tree.npz, recorded from src/tree.cpp and src/particles.cpp compiled where
+    they lie): keys, particle ranges, leaf flags, depths, centres, radius bits, boxes and the
+    particle order bit for bit; the maximum-depth error where the reference stops with it."""
+    import cosmictiger_b200 as ct
+
+    d = REF_TREE
+    x, y, z = (d[case + "/in"][k].copy() for k in range(3))
+    theta, hsoft, bucket = (float(q) for q in d[case + "/params"])
+    n = len(x)
+    box = ctx.box(n)
+    box.upload(x, y, z, np.zeros((n, 3), np.float32), np.zeros(n, np.int8))
+    if bool(d[case + "/threw"]):
+        with pytest.raises(ct.GravityError, match="depth"):
+            box.tree_create(theta, hsoft, int(bucket))
+        box.close()
+        return
+    box.tree_create(theta, hsoft, int(bucket))
+    nodes = box.tree()
+    out = box.download()
+    box.close()
+    after = d[case + "/after"]
+    assert np.array_equal(out["x"], after[0]) and np.array_equal(out["y"], after[1]) and np.array_equal(out["z"], after[2])
+    ref = {f: d[case + "/" + f] for f in ("key", "part_begin", "part_end", "leaf", "depth", "pos", "box_begin", "box_end", "radius")}
+    assert len(nodes) == len(ref["key"])
+    a = nodes[np.argsort(nodes["key"], kind="stable")]
+    o = np.argsort(ref["key"], kind="stable")
+    assert np.array_equal(a["key"], ref["key"][o])
+    for f in ("part_begin", "part_end", "leaf", "depth", "pos", "box_begin", "box_end"):
+        assert np.array_equal(a[f], ref[f][o]), f
+    assert np.array_equal(a["radius"].view(np.uint32), ref["radius"][o].view(np.uint32)), "radius"
 
 
 # Potentials of a periodic box are small residuals of two large sums (the softened direct
