@@ -9,7 +9,9 @@ positions, the IEEE build's tree (ct_or_node fields: heap keys, particle ranges,
 centres, radii, boxes, leaf flags, depths) and particle order, and how far the native build's
 centres (in units of 2^-32) and radii (in units in the last place) are from them -- its keys,
 ranges, boxes, leaf flags, depths and particle order are required to be the same; a case where the reference throws (more than a bucket of coincident particles,
-"Maximum depth exceeded", tree.cpp:285-286) records the error instead.
+"Maximum depth exceeded", tree.cpp:285-286) records the error instead.  The same probe runs
+the reference's rung partition (particles_sort_by_rung with push/pop of the active range,
+src/particles.cpp:218-235,1029-1076) through RUNG_OPS on seeded particles ("rungs/..." entries).
 
     python tests/golden/make_tree_golden.py            # writes tests/golden/ref_tree.npz
     python tests/golden/make_tree_golden.py --check    # compares a fresh recording with it
@@ -30,6 +32,10 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 OUT = os.path.join(HERE, "ref_tree.npz")
+# the rung partition's operation sequence: minimum rungs of particles_sort_by_rung, with the
+# active-range stack of particles_push_rungs / particles_pop_rungs between them (a ladder of
+# the kind kick_step_hierarchical runs, driver.cpp:382-593, and some restarts from wider ranges)
+RUNG_OPS = ["1", "push", "2", "push", "3", "push", "4", "pop", "pop", "3", "pop", "2", "0", "2", "push", "5", "pop", "1"]
 PROBE = os.path.join(ROOT, "oracle", "_ref", "tree_probe")
 PROBE_NATIVE = os.path.join(ROOT, "oracle", "_ref", "tree_probe_native")
 FIELDS = ("key", "part_begin", "part_end", "child_left", "child_right", "pos", "radius", "box_begin", "box_end", "leaf", "depth")
@@ -90,8 +96,51 @@ def run_probe(probe, x, y, z, theta, hsoft, bucket):
     return nodes, after
 
 
+def rung_case():
+    """1,500 particles with rungs 0-5 (more on the low rungs), seeded positions and velocities."""
+    rng = np.random.default_rng(31)
+    n = 1500
+    x, y, z = (rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32) for _ in range(3))
+    v = rng.standard_normal((n, 3)).astype(np.float32)
+    r = np.minimum(rng.geometric(0.45, n) - 1, 5).astype(np.int8)
+    return x, y, z, v, r
+
+
+def run_rungs(probe, x, y, z, v, r, ops):
+    """The reference's rung partition: (active-range start after each op, x, y, z, v, rung)."""
+    n = len(x)
+    with tempfile.TemporaryDirectory() as tmp:
+        fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+        with open(fin, "wb") as f:
+            np.array([n], np.int64).tofile(f)
+            for a in (x, y, z):
+                np.ascontiguousarray(a, np.uint32).tofile(f)
+            np.ascontiguousarray(v, np.float32).tofile(f)
+            np.ascontiguousarray(r, np.int8).tofile(f)
+        res = subprocess.run([probe, "--rungs", fin, fout] + list(ops), capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError("rung probe failed (%d): %s" % (res.returncode, res.stderr[-400:]))
+        with open(fout, "rb") as f:
+            cnt = int(np.fromfile(f, np.int64, 1)[0])
+            begins = np.fromfile(f, np.int64, cnt)
+            xs = [np.fromfile(f, np.uint32, n) for _ in range(3)]
+            vs = np.fromfile(f, np.float32, 3 * n).reshape(n, 3)
+            rs = np.fromfile(f, np.int8, n)
+    return begins, xs, vs, rs
+
+
 def record():
     data = {}
+    x, y, z, v, r = rung_case()
+    begins, xs, vs, rs = run_rungs(PROBE, x, y, z, v, r, RUNG_OPS)
+    data["rungs/in_x"] = np.stack([x, y, z])
+    data["rungs/in_v"] = v
+    data["rungs/in_rung"] = r
+    data["rungs/ops"] = np.array(RUNG_OPS)
+    data["rungs/begins"] = begins
+    data["rungs/x"] = np.stack(xs)
+    data["rungs/v"] = vs
+    data["rungs/rung"] = rs
     for name, x, y, z, theta, hsoft, bucket in cases():
         data[name + "/in"] = np.stack([x, y, z])
         data[name + "/params"] = np.array([theta, hsoft, bucket], np.float64)

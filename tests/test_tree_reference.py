@@ -9,7 +9,9 @@ give the IEEE build's tree bit for bit -- heap keys, particle ranges, children, 
 boxes, leaf flags, depths, particle order -- and the native build's keys, ranges, boxes, leaf
 flags, depths and order, with its centres and radii within what its contracted arithmetic
 changes.  The case with more than a bucket of coincident particles must stop with the
-reference's "Maximum depth exceeded".
+reference's "Maximum depth exceeded".  The same file holds the reference's rung partition
+(particles_sort_by_rung with push/pop of the active range, src/particles.cpp:218-235,
+1029-1076) over a sequence of operations, which O1 must reproduce exactly.
 """
 import os
 import subprocess
@@ -28,7 +30,7 @@ FIELDS = ("key", "part_begin", "part_end", "child_left", "child_right", "pos", "
 
 def fixture_cases():
     d = np.load(FIX)
-    return sorted({k.split("/")[0] for k in d.files})
+    return sorted({k.split("/")[0] for k in d.files} - {"rungs"})
 
 
 @pytest.fixture(scope="module")
@@ -82,3 +84,24 @@ def test_fixture_equals_a_fresh_run_of_the_reference():
     committed fixture (guards the fixture against drift of the generator or the probe)."""
     res = subprocess.run([sys.executable, os.path.join(HERE, "golden", "make_tree_golden.py"), "--check"], capture_output=True, text=True, cwd=ROOT)
     assert res.returncode == 0, res.stdout + res.stderr
+
+
+def test_oracle_rung_partition_equals_reference(fix, oracle):
+    """O1's rung partition and an active-range stack give the reference's range starts after
+    every operation and its final particle order, velocities and rungs, bit for bit."""
+    x, y, z = (fix["rungs/in_x"][k].copy() for k in range(3))
+    v = fix["rungs/in_v"].copy()
+    r = fix["rungs/in_rung"].copy()
+    begin, stack, got = 0, [], []
+    for op in fix["rungs/ops"]:
+        if op == "push":
+            stack.append(begin)
+        elif op == "pop":
+            begin = stack.pop()
+        else:
+            m = int(op)
+            begin = 0 if m == 0 else oracle.sort_by_rung(x, y, z, v, r, m, begin)
+        got.append(begin)
+    assert got == [int(b) for b in fix["rungs/begins"]]
+    assert np.array_equal(np.stack([x, y, z]), fix["rungs/x"])
+    assert np.array_equal(v, fix["rungs/v"]) and np.array_equal(r, fix["rungs/rung"])
