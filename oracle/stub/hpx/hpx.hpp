@@ -255,11 +255,15 @@ inline void this_thread_yield() {
 }
 }  // namespace hpx
 
-// an action calls its function directly (one locality)
-#define HPX_PLAIN_ACTION(f)                                                   \
-	struct f##_action {                                                         \
+// an action calls its function directly (one locality); HPX_PLAIN_ACTION(f) names it f_action,
+// HPX_PLAIN_ACTION(f, name) names it name
+#define HPX_PLAIN_ACTION_NAMED(f, name)                                       \
+	struct name {                                                               \
 		template<class... A>                                                    \
 		auto operator()(A&&... a) const -> decltype(f(std::forward<A>(a)...)) { \
 			return f(std::forward<A>(a)...);                                      \
 		}                                                                       \
 	}
+#define HPX_PLAIN_ACTION_1(f) HPX_PLAIN_ACTION_NAMED(f, f##_action)
+#define HPX_PLAIN_ACTION_PICK(_1, _2, which, ...) which
+#define HPX_PLAIN_ACTION(...) HPX_PLAIN_ACTION_PICK(__VA_ARGS__, HPX_PLAIN_ACTION_NAMED, HPX_PLAIN_ACTION_1, unused)(__VA_ARGS__)
