@@ -47,8 +47,8 @@ CT_HD_FN int ct_ffs(unsigned int m) {
 	return __builtin_ffs((int) m);
 #endif
 }
-CT_HD_FN unsigned int ct_word6(const unsigned int* a, int w) {
-	return w == 0 ? a[0] : w == 1 ? a[1] : w == 2 ? a[2] : w == 3 ? a[3] : w == 4 ? a[4] : a[5];
+CT_HD_FN unsigned int ct_word4(const unsigned int* a, int w) {
+	return w == 0 ? a[0] : w == 1 ? a[1] : w == 2 ? a[2] : a[3];
 }
 CT_HD_FN float ct_sqrt(float a) {
 #ifdef __CUDA_ARCH__

@@ -594,7 +594,20 @@ def gen_header(P):
     h.append("static constexpr double ERF_SERIES_H[ORDER][ERF_SERIES_N] = {%s};" % body)
     h.append("#ifdef __CUDACC__")
     h.append("static __constant__ double ERF_SERIES_D[ORDER][ERF_SERIES_N] = {%s};" % body)
+    h.append("// the same coefficients rounded to float once, for the single-precision evaluation")
+    h.append("static __constant__ float ERF_SERIES_DF[ORDER][ERF_SERIES_N] = {%s};" % body)
     h.append("#endif")
+    h.append("template<class T> CT_HD T erf_series(int l, int j) {")
+    h.append("#ifdef __CUDA_ARCH__")
+    h.append("\tif constexpr (sizeof(T) == sizeof(float)) {")
+    h.append("\t\treturn ERF_SERIES_DF[l][j];")
+    h.append("\t} else {")
+    h.append("\t\treturn T(ERF_SERIES_D[l][j]);")
+    h.append("\t}")
+    h.append("#else")
+    h.append("\treturn T(ERF_SERIES_H[l][j]);")
+    h.append("#endif")
+    h.append("}")
     # Fourier accumulation unrolled: odd-order entries take the sine, even ones the cosine
     acc = "\n".join("\t\tD[%d] = ct_fma(%s, T(tab.four_exp[i][%d]), D[%d]);" % (kk, "sn" if sum(n) & 1 else "cn", kk, kk)
                     for kk, n in enumerate(tl_stored(P)))
@@ -633,9 +646,9 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 			T zl = T(1);
 			T bl = T(2e-3);
 			for (int l = 0; l < ORDER; l++) {
-				T s = T(CT_TAB(ERF_SERIES)[l][ERF_SERIES_N - 1]);
+				T s = erf_series<T>(l, ERF_SERIES_N - 1);
 				for (int j = ERF_SERIES_N - 2; j >= 0; j--) {
-					s = ct_fma(s, w, T(CT_TAB(ERF_SERIES)[l][j]));
+					s = ct_fma(s, w, erf_series<T>(l, j));
 				}
 				g[l] = bl * zl * s;
 				zl *= zz;
@@ -675,7 +688,7 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 	for (int q = 0; q < nin; q++) {
 		while (bits == 0u) {
 			wd++;
-			bits = ct_word6(inside, wd);
+			bits = ct_word4(inside, wd);
 		}
 		const int i = 32 * wd + ct_ffs(bits) - 1;
 		bits &= bits - 1u;
