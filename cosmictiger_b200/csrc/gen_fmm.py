@@ -718,6 +718,7 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 	// h, so every entry's product is unchanged): the first half of the table holds one vector
 	// of each pair (ewald_build_indices), taken twice.
 	static_assert(CT_EWALD_NFOUR % 2 == 0, "Fourier vectors come in +h/-h pairs");
+#pragma unroll 1
 	for (int i = 0; i < CT_EWALD_NFOUR / 2; i++) {
 		const T hdotx = ct_fma(T(tab.four[i][0]), x, ct_fma(T(tab.four[i][1]), y, T(tab.four[i][2]) * z));
 		T sn, cn;
