@@ -199,15 +199,45 @@ CT_HD_FN void ct_sincos_poly(double x, double* s, double* c) {
 }
 
 // erfc(x) and exp(-x^2) by Abramowitz & Stegun 7.1.26 (|error| <= 1.5e-7), the form the
-// reference uses on the device (cosmictiger/math.hpp:56-71).
+// reference uses on the device (cosmictiger/math.hpp:56-71).  On the device, in single
+// precision, the reciprocal and the exponential are CUDA's fast intrinsics (__fdividef,
+// __expf: a few ulp, far below the formula's own error), as the reference's --use_fast_math
+// build makes them; the host keeps the correctly rounded division and its own exponential.
 template<class T>
 CT_HD_FN void ct_erfcexp(T x, T* ec, T* ex) {
 	const T p = T(0.3275911), a1 = T(0.254829592), a2 = T(-0.284496736), a3 = T(1.421413741), a4 = T(-1.453152027), a5 = T(1.061405429);
+#ifdef __CUDA_ARCH__
+	T t;
+	if constexpr (sizeof(T) == sizeof(float)) {
+		t = __fdividef(1.0f, ct_fma(p, x, T(1)));
+		*ex = __expf(-x * x);
+	} else {
+		t = T(1) / ct_fma(p, x, T(1));
+		*ex = ct_exp_poly(-x * x);
+	}
+#else
 	const T t = T(1) / ct_fma(p, x, T(1));
 	*ex = ct_exp_poly(-x * x);
+#endif
 	T s = ct_fma(a5, t, a4);
 	s = ct_fma(s, t, a3);
 	s = ct_fma(s, t, a2);
 	s = ct_fma(s, t, a1);
 	*ec = s * t * *ex;
+}
+
+// distance and its reciprocal from the squared distance (> 0): on the device in single
+// precision one MUFU reciprocal square root and a product, elsewhere the correctly rounded
+// square root and division
+template<class T>
+CT_HD_FN void ct_dist(T r2, T* r, T* rinv) {
+#ifdef __CUDA_ARCH__
+	if constexpr (sizeof(T) == sizeof(float)) {
+		*rinv = rsqrtf(r2);
+		*r = r2 * *rinv;
+		return;
+	}
+#endif
+	*r = ct_sqrt(r2);
+	*rinv = T(1) / *r;
 }

@@ -291,21 +291,25 @@ def gen_radial(P, stf_from=3):
     zero, so the stored tensor after the projection is the same."""
     em = Emitter()
     full = full_set(P)
-    def terms_of(n):
-        return [(0, 0, 0)] if sum(n) >= stf_from else list(half_range(n))
-
+    low = [n for n in full if sum(n) < stf_from]
+    high = [n for n in full if sum(n) >= stf_from]
+    # orders below stf_from: every term; orders from stf_from on: u^n g_N, formed as
+    # (ux^a uy^b) (g_N uz^c), which shares the xy monomials and the z powers across orders
     needed = set()
-    for n in full:
-        for m in terms_of(n):
+    for n in low:
+        for m in half_range(n):
             needed.add(sub(n, add(m, m)))
+    for n in high:
+        needed.add((n[0], n[1], 0))
+        needed.add((0, 0, n[2]))
     mon = monomials(em, "u", "ux", "uy", "uz", needed)
     em("const T ri1 = rinv;")
     for k in range(2, P // 2 + 1):
         em("const T ri%d = ri%d * rinv;" % (k, k - 1))
     pw = {}
-    for n in full:
+    for n in low:
         N = sum(n)
-        for m in terms_of(n):
+        for m in half_range(n):
             m0 = sum(m)
             pw[(N - m0, m0)] = True
     for (l, m0) in sorted(pw):
@@ -313,10 +317,21 @@ def gen_radial(P, stf_from=3):
             em("const T G%d_%d = g%d;" % (l, m0, l))
         else:
             em("const T G%d_%d = g%d * ri%d;" % (l, m0, l, m0))
+    zs = sorted({(sum(n), n[2]) for n in high})
+    for (N, c) in zs:
+        em("const T Z%d_%d = %s;" % (N, c, "g%d" % N if c == 0 else "g%d * %s" % (N, mon[(0, 0, c)])))
     for n in full:
         N = sum(n)
+        if N >= stf_from:
+            xy = mon[(n[0], n[1], 0)]
+            z = "Z%d_%d" % (N, n[2])
+            if xy == "T(1)":
+                em("Dr[%d] = (Dr[%d] + %s);" % (sym_index(n), sym_index(n), z))
+            else:
+                em("Dr[%d] = ct_fma(%s, %s, Dr[%d]);" % (sym_index(n), xy, z, sym_index(n)))
+            continue
         terms = []
-        for m in terms_of(n):
+        for m in half_range(n):
             m0 = sum(m)
             c = Fr(vfact(n), (2 ** m0) * vfact(m) * vfact(sub(n, add(m, m))))
             terms.append((c, (mon[sub(n, add(m, m))], "G%d_%d" % (N - m0, m0))))
@@ -698,8 +713,8 @@ template<class T, class Tab> CT_HD int ewald_greens(T* __restrict__ D, T x, T y,
 			const T dz = z - T(1000) * T(tab.real[i][2]);
 			const T r2 = ct_fma(dx, dx, ct_fma(dy, dy, dz * dz));
 			icnt++;
-			const T r = ct_sqrt(r2);
-			const T rinv = T(1) / r;
+			T r, rinv;
+			ct_dist(r2, &r, &rinv);
 			T ec, ex;
 			ct_erfcexp(T(2e-3) * r, &ec, &ex);
 			T e0 = T(2.2567583341910252e-3) * ex * rinv;

@@ -5,7 +5,8 @@ oracle/ladder_probe.cpp (`make -C oracle ladder`) runs the reference's kick_step
 STEPS steps on a seeded clustered box; its kick and drift are this project's CPU restatement
 (oracle/libct_oracle.so, pinned against the reference's CUDA kernels elsewhere).  The fixture
 holds the input state and parameters, after each step the ladder's minimum rung, maximum rung
-and active-range start with a SHA-256 digest of the particle state, and the final state.
+and active-range start with a SHA-256 digest of the particle state, the final state, and a
+digest of the oracle sources it was recorded with (re-record when they change).
 
     python tests/golden/make_ladder_golden.py            # writes tests/golden/ref_ladder.npz
     python tests/golden/make_ladder_golden.py --check    # compares a fresh recording with it
@@ -27,6 +28,16 @@ sys.path.insert(0, os.path.dirname(HERE))
 OUT = os.path.join(HERE, "ref_ladder.npz")
 PROBE = os.path.join(ROOT, "oracle", "_ref", "ladder_probe")
 STEPS = 4
+
+
+def oracle_digest():
+    """SHA-256 of the sources of the oracle's kick and drift (the probe's stand-ins for the
+    reference's GPU calls): a fixture recorded with other sources no longer applies."""
+    h = hashlib.sha256()
+    for f in ("cosmictiger_b200/csrc/fmm_p7.h", "cosmictiger_b200/csrc/fmm_common.h", "oracle/ct_oracle.cpp"):
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return np.frombuffer(h.digest(), np.uint8)
 
 
 def state_digest(x, y, z, v, r):
@@ -87,6 +98,7 @@ def record():
     data["final_x"] = np.stack(xs)
     data["final_v"] = vs
     data["final_rung"] = rs
+    data["oracle_digest"] = oracle_digest()
     return data
 
 
