@@ -54,10 +54,10 @@ def parse():
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own CUDA kick on the same box")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shape instead of autotuning it first")
     ap.add_argument("--accuracy-sinks", type=int, default=10000, help="FP64 direct-Ewald check on this many seeded sinks (0: skip)")
-    ap.add_argument("--ensemble-boxes", type=int, default=64, help="boxes of the batched-vs-plain ensemble comparison (0: skip)")
+    ap.add_argument("--ensemble-boxes", type=int, default=512, help="boxes of the batched-vs-plain ensemble comparison (0: skip)")
     ap.add_argument("--ensemble-nmin", type=int, default=16)
-    ap.add_argument("--ensemble-nmax", type=int, default=64)
-    ap.add_argument("--ensemble-steps", type=int, default=3)
+    ap.add_argument("--ensemble-nmax", type=int, default=128)
+    ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--study", default="none", choices=["none", "precision", "ensemble", "serving", "lightcone", "fourier", "autotune"],
                     help="instead of the benchmark line: precision (theta x order x summation, force error vs FP64 Ewald and "
                          "particle-steps/s), ensemble (512 boxes of 16^3..128^3, batched vs box by box, 20 steps) or serving "
@@ -81,8 +81,13 @@ def make_ensemble(nbox, nmin, nmax, seed):
     ns = np.rint(np.exp(rng.uniform(np.log(nmin), np.log(nmax), nbox))).astype(int)
     idx = rng.uniform(-2.5, -1.0, nbox)
     rms = rng.uniform(0.1, 0.6, nbox)
-    boxes = [ics.zeldovich_lattice(int(n), index=float(i), rms_spacing=float(r), seed=int(seed * 1000 + k)) for k, (n, i, r) in enumerate(zip(ns, idx, rms))]
-    return boxes
+    jobs = [(int(n), float(i), float(r), int(seed * 1000 + k)) for k, (n, i, r) in enumerate(zip(ns, idx, rms))]
+    # every box has its own seed, so the threads' order does not change the result; numpy's
+    # FFTs release the interpreter lock, so the host's cores share the generation
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1))) as ex:
+        return list(ex.map(lambda j: ics.zeldovich_lattice(j[0], index=j[1], rms_spacing=j[2], seed=j[3]), jobs))
 
 
 def ensemble_compare(ct, torch, ctx, args, theta, lib_stream):
@@ -98,6 +103,32 @@ def ensemble_compare(ct, torch, ctx, args, theta, lib_stream):
     t0 = 1.0 / 64
     hs = np.array([ics.softening(n, 0.02) for n in counts], np.float32)
     gms = np.array([1.0 / n for n in counts], np.float32)
+    # the launch shape tuned for this workload (the first 128 boxes of the set, batched; 12
+    # candidates, timing only), used by both paths and put back afterwards
+    prev_shape = ctx.tuning()
+    shape = None
+    if not args.no_tune:
+        from cosmictiger_b200 import autotune
+
+        nt = min(len(sets), 128)
+        tc = counts[:nt]
+        tcat = [np.concatenate([s[k] for s in sets[:nt]]) for k in range(5)]
+
+        def factory():
+            e = ctx.ensemble(tc)
+            e.upload(*tcat)
+            e.set_box_params(hs[:nt], gms[:nt])
+            return e
+
+        try:
+            tr = autotune.tune(ctx, tcat, theta=theta, h=float(hs[:nt].max()), buckets=(128,), max_force_rms=None, repeats=1, box_factory=factory,
+                               forces=False)
+            shape = {"chosen": {k: tr["best"][k] for k in ("p2p_stage", "warps_per_tile", "tile_width")}, "ms_kick_chosen": tr["best"]["ms"],
+                     "ms_kick_default": tr["reference"]["ms"], "candidates": len(tr["rows"]), "tuned_on": "the first %d boxes, batched" % nt}
+        except Exception as e:  # reported; both paths then run at the context's shape
+            ctx.set_tuning(prev_shape["p2p_stage"], prev_shape["warps_per_tile"], prev_shape["tile_width"])
+            shape = {"failed": str(e), **prev_shape}
+        del tcat
     ens = ctx.ensemble(counts)
     ens.upload(*[np.concatenate([s[k] for s in sets]) for k in range(5)])
     ens.set_box_params(hs, gms)
@@ -152,9 +183,11 @@ def ensemble_compare(ct, torch, ctx, args, theta, lib_stream):
     for bx in plain:
         bx.close()
     ens.close()
+    ctx.set_tuning(prev_shape["p2p_stage"], prev_shape["warps_per_tile"], prev_shape["tile_width"])
     vb = N * K / (ms_b / 1e3)
     vp = N * K / (ms_p / 1e3)
     return {"boxes": len(counts), "particles": N, "n_range": [args.ensemble_nmin, args.ensemble_nmax], "steps": K,
+            "launch_shape": shape if shape else prev_shape,
             "batched_particle_steps_s": vb, "plain_particle_steps_s": vp, "speedup": vb / vp,
             "batched_ms_per_step": ms_b / K, "batched_last_kick": breakdown, "plain_box_ms_p50": float(np.percentile(lat, 50)), "plain_box_ms_p99": float(np.percentile(lat, 99))}
 
@@ -940,17 +973,13 @@ def study_precision(args, torch):
 
 def study_ensemble(args, torch):
     """512 independent boxes, n_i log-uniform in [16, 128], own Zel'dovich fields, theta 0.55,
-    20 steps (or the --ensemble-* sizes when given): one batched ensemble vs the plain
-    single-box path launched box by box."""
+    20 steps (the --ensemble-* defaults, or the sizes given): one batched ensemble vs the plain
+    single-box path launched box by box, without the benchmark line around it."""
     import cosmictiger_b200 as ct
 
     ctx = ct.Context(order=7)
     lib_stream = torch.cuda.ExternalStream(ctx.lib.ct_stream(ctx.h))
-    a = argparse.Namespace(**vars(args))
-    if (args.ensemble_boxes, args.ensemble_nmin, args.ensemble_nmax, args.ensemble_steps) == (64, 16, 64, 3):
-        # sizes left at the benchmark line's defaults: the study's own configuration
-        a.ensemble_boxes, a.ensemble_nmin, a.ensemble_nmax, a.ensemble_steps = 512, 16, 128, 20
-    res = ensemble_compare(ct, torch, ctx, a, args.theta, lib_stream)
+    res = ensemble_compare(ct, torch, ctx, args, args.theta, lib_stream)
     ctx.close()
     return {"study": "ensemble", **res}
 
@@ -1128,7 +1157,7 @@ def study_autotune(args, torch):
     res = autotune.tune(ctx, state, theta=args.theta, h=ics.softening(N, 0.02), buckets=(64, 96, 128, 160, 192), max_force_rms=None, repeats=2)
     out["single_box"] = {"workload": workload_name(args).replace("4-rung hierarchical steps", "all-particles kick"), **res}
     print(json.dumps({"single_box_best": res["best"], "reference": res["reference"]}), flush=True)
-    nb = args.ensemble_boxes if args.ensemble_boxes != 64 else 128
+    nb = args.ensemble_boxes if args.ensemble_boxes != 512 else 128
     sets = make_ensemble(nb, 16, 128, seed=4)
     counts = [len(s[0]) for s in sets]
     cat = [np.concatenate([s[k] for s in sets]) for k in range(5)]

@@ -83,18 +83,22 @@ SHAPES = tuple((s, w, t) for s in (64, 128, 256) for w in (1, 2) for t in (32, 1
 
 
 def tune(ctx, state, theta=0.55, h=None, buckets=(128,), shapes=SHAPES, reference=(128, (128, 1, 32)), max_force_rms=1e-5, repeats=2,
-         box_factory=None):
+         box_factory=None, forces=True):
     """Joint search over leaf sizes and launch shapes (p2p_stage, warps_per_tile, tile_width).
     Every candidate runs repeats + 1 times (the first untimed) on the state uploaded again each
     time; the time is the library's device time of the kick's phases (tree build included).
     Forces are compared with the reference candidate's (particles matched by position);
     max_force_rms None keeps every candidate.  box_factory() (default ctx.box(n)) makes the box
-    the candidates run on, e.g. an ensemble with its per-box parameters set.  Leaves the context at the chosen shape; returns
-    {"best": {...}, "reference": {...}, "rows": [...]}."""
+    the candidates run on, e.g. an ensemble with its per-box parameters set.  forces=False times
+    the candidates only (no force download or comparison, force_rms None; max_force_rms must be
+    None): for launch shapes alone, which change the forces only by rounding.  Leaves the context
+    at the chosen shape; returns {"best": {...}, "reference": {...}, "rows": [...]}."""
     from . import KickParams
 
     if repeats < 1:
         raise ValueError("repeats must be >= 1 (the first run of each candidate is not timed)")
+    if not forces and max_force_rms is not None:
+        raise ValueError("a force bound needs the forces (forces=True)")
     x, y, z, v, r = state
     n = len(x)
     h = ics.softening(n, 0.02) if h is None else h
@@ -117,11 +121,11 @@ def tune(ctx, state, theta=0.55, h=None, buckets=(128,), shapes=SHAPES, referenc
             for rep in range(repeats + 1):
                 box.upload(x, y, z, v, r)
                 box.tree_create(theta, h, bucket)
-                box.kick(KickParams.make(theta=theta, h=h, GM=1.0 / n, eta=ics.eta_default(), t0=1.0 / 64, first_call=True, save_force=True))
+                box.kick(KickParams.make(theta=theta, h=h, GM=1.0 / n, eta=ics.eta_default(), t0=1.0 / 64, first_call=True, save_force=forces))
                 c = box.counters()
                 if rep > 0:
                     times.append(sum(c[p] for p in PHASES))
-                if rep == repeats:
+                if forces and rep == repeats:
                     out = box.download(forces=True)
                     if bucket not in order_of:
                         order_of[bucket] = (out["x"].copy(), np.lexsort((out["z"], out["y"], out["x"])))
@@ -130,10 +134,10 @@ def tune(ctx, state, theta=0.55, h=None, buckets=(128,), shapes=SHAPES, referenc
                         raise RuntimeError("the tree order changed between launch shapes of one leaf size")
                     g = np.stack([out["gx"][order], out["gy"][order], out["gz"][order]], axis=1).astype(np.float64)
                     del out
-            if ref is None:
+            if forces and ref is None:
                 ref = g
             rows.append({"bucket": bucket, "p2p_stage": shape[0], "warps_per_tile": shape[1], "tile_width": shape[2], "ms": float(min(times)),
-                         "force_rms": float(np.sqrt(np.sum((g - ref) ** 2) / np.sum(ref ** 2)))})
+                         "force_rms": float(np.sqrt(np.sum((g - ref) ** 2) / np.sum(ref ** 2))) if forces else None})
     finally:
         box.close()
     ok = [row for row in rows if max_force_rms is None or row["force_rms"] <= max_force_rms]

@@ -148,3 +148,29 @@ def test_tune_picks_the_fastest_shape_within_the_force_tolerance():
     res2 = autotune.tune(ctx2, state, h=1e-3, buckets=(96, 128, 160), shapes=list(SHAPE_TIME), max_force_rms=None)
     assert (res2["best"]["bucket"], res2["best"]["p2p_stage"], res2["best"]["warps_per_tile"], res2["best"]["tile_width"]) == (160, 128, 1, 16)
     assert len(res2["rows"]) == 3 * len(SHAPE_TIME)
+
+
+def test_tune_timing_only_downloads_nothing():
+    """forces=False times the launch shapes without saving or downloading forces (the box's
+    download raises if it is reached), still picks the fastest and leaves it set; a force bound
+    without the forces is refused before any device work."""
+    class NoDownload(ShapeBox):
+        def download(self, forces=False):
+            raise AssertionError("timing-only tuning downloaded the state")
+
+    class Ctx(ShapeCtx):
+        def box(self, n):
+            return NoDownload(self, n)
+
+    n = 300
+    rng = np.random.default_rng(4)
+    state = [rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32) for _ in range(3)] + [np.zeros((n, 3), np.float32), np.zeros(n, np.int8)]
+    ctx = Ctx()
+    res = autotune.tune(ctx, state, h=1e-3, shapes=list(SHAPE_TIME), max_force_rms=None, repeats=1, forces=False)
+    best = (res["best"]["p2p_stage"], res["best"]["warps_per_tile"], res["best"]["tile_width"])
+    assert best == (128, 1, 16) and ctx.shape == best
+    assert all(r["force_rms"] is None for r in res["rows"])
+    ctx2 = Ctx()
+    with pytest.raises(ValueError):
+        autotune.tune(ctx2, state, h=1e-3, max_force_rms=1e-5, forces=False)
+    assert not ctx2.set_calls
