@@ -79,21 +79,25 @@ const char* cudaGetErrorString(cudaError_t) {
 	return "tree_probe: no CUDA";
 }
 }
-// the reference's random initial conditions and sampler are not reached
-const gsl_rng_type* gsl_rng_taus = nullptr;
-gsl_rng* gsl_rng_alloc(const gsl_rng_type*) {
+// the reference's random initial conditions and sampler are not reached by the tree and ladder
+// probes; weak, so that the initial-condition probe (oracle/ic_probe.cpp) supplies the generator
+__attribute__((weak)) const gsl_rng_type* gsl_rng_taus = nullptr;
+__attribute__((weak)) gsl_rng* gsl_rng_alloc(const gsl_rng_type*) {
 	abort();
 }
-void gsl_rng_set(const gsl_rng*, unsigned long int) {
+__attribute__((weak)) void gsl_rng_set(const gsl_rng*, unsigned long int) {
 	abort();
 }
-double gsl_rng_uniform(const gsl_rng*) {
+__attribute__((weak)) double gsl_rng_uniform(const gsl_rng*) {
 	abort();
 }
-unsigned long int gsl_rng_get(const gsl_rng*) {
+__attribute__((weak)) double gsl_rng_uniform_pos(const gsl_rng*) {
 	abort();
 }
-void gsl_rng_free(gsl_rng*) {
+__attribute__((weak)) unsigned long int gsl_rng_get(const gsl_rng*) {
+	abort();
+}
+__attribute__((weak)) void gsl_rng_free(gsl_rng*) {
 	abort();
 }
 

@@ -9,5 +9,6 @@ extern const gsl_rng_type* gsl_rng_taus;
 gsl_rng* gsl_rng_alloc(const gsl_rng_type*);
 void gsl_rng_set(const gsl_rng*, unsigned long int);
 double gsl_rng_uniform(const gsl_rng*);
+double gsl_rng_uniform_pos(const gsl_rng*);
 unsigned long int gsl_rng_get(const gsl_rng*);
 void gsl_rng_free(gsl_rng*);
