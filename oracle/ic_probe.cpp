@@ -1,8 +1,10 @@
 // Test infrastructure only (oracle build; never part of the library).
 //
 // Runs the reference's own initial-condition generator, initialize() of src/initialize.cpp
-// (Zel'dovich displacements and the 2LPT correction, src/initialize.cpp:261-355,436-898), with
-// its distributed 3-D transform (src/fft.cpp) compiled where they lie, in one process: HPX is
+// (Zel'dovich displacements and the 2LPT correction, src/initialize.cpp:261-355,436-898), and its
+// matter power spectrum, power_spectrum_compute() of src/power.cpp with the binning of
+// src/fft.cpp:172-360 and the density kernel of src/power.cu:31-67, with its distributed 3-D
+// transform (src/fft.cpp) compiled where they lie, in one process: HPX is
 // the single-threaded stand-in in stub/hpx, FFTW's one-line transforms are the plain discrete
 // Fourier sums below (double accumulation, stored in single precision as FFTW stores them),
 // GSL's "taus" generator is L'Ecuyer's published three-component Tausworthe recurrence (the
@@ -10,17 +12,21 @@
 // working directory, as the reference reads it (src/initialize.cpp:870-898).
 //
 //   ic_probe N box_mpc z0 omega_m hubble sigma8 twolpt table.txt out.bin
+//   ic_probe power N fold box_mpc particles.bin out.bin
 //
 // table.txt holds "k P" lines (k in h/Mpc, P in (Mpc/h)^3); the probe copies it to ./power.init.
 // out.bin: int64 n, then n uint32 x, y, z (fixed32 raw), then n float vx, vy, vz, then the
 // float factors D1, D2, prefac1, prefac2 as initialize() computes them for z0.
 // Code units: box = 1, H0 = 1 (code_to_s = 1 / (H0 [1/s] * hubble)).
+// power mode: particles.bin holds int64 n, then n uint32 x, y, z (fixed32 raw); out.bin gets
+// int64 m, then m float k, P, Perr (the power_spectrum_t the reference returns).
 #include "ref_host.h"
 
 #include <cosmictiger/boltzmann.hpp>
 #include <cosmictiger/constants.hpp>
 #include <cosmictiger/cosmology.hpp>
 #include <cosmictiger/initialize.hpp>
+#include <cosmictiger/power.hpp>
 #include <cosmictiger/zero_order.hpp>
 #include <fftw3.h>
 #include <silo.h>
@@ -28,6 +34,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 // ---------------------------------------------------------------- GSL "taus" (L'Ecuyer 1996)
@@ -170,6 +177,50 @@ void fftwf_destroy_plan(fftwf_plan p) {
 	delete p;
 }
 
+// ---------------------------------------------------------------- the density kernel
+// The reference's accumulate_density_kernel (src/power.cu:31-67), taken verbatim from its
+// source into oracle/_ref/ic/power_kernel.inc by the build recipe, compiled here as a host
+// function: its launch indices are the emulated block and thread below, and its atomic adds
+// plain adds (one thread at a time).
+namespace emu {
+struct index3 {
+	unsigned x = 0, y = 0, z = 0;
+};
+static index3 thread, block, grid;
+}  // namespace emu
+static inline float emu_atomic_add(float* p, float v) {
+	const float old = *p;
+	*p = old + v;
+	return old;
+}
+#undef __global__
+#define __global__ static
+#define threadIdx emu::thread
+#define blockIdx emu::block
+#define gridDim emu::grid
+#define atomicAdd emu_atomic_add
+#define BLOCK_SIZE 256
+#include "power_kernel.inc"
+#undef threadIdx
+#undef blockIdx
+#undef gridDim
+#undef atomicAdd
+
+// The reference's launch wrapper (src/power.cu:69-84) on the host: a zeroed density box and
+// the kernel over one block of BLOCK_SIZE threads, run thread by thread (the GPU's order of the
+// atomic adds is not fixed either; sums differ by rounding only).
+vector<float> accumulate_density_cuda(int M, int Ndim, range<int64_t> intbox) {
+	vector<float> rho(intbox.volume(), 0.f);
+	emu::grid.x = 1;
+	emu::block.x = 0;
+	for (unsigned t = 0; t < BLOCK_SIZE; t++) {
+		emu::thread.x = t;
+		accumulate_density_kernel(&particles_pos(XDIM, 0), &particles_pos(YDIM, 0), &particles_pos(ZDIM, 0), rho.data(), M, particles_size(), Ndim,
+				intbox);
+	}
+	return rho;
+}
+
 // ---------------------------------------------------------------- not reached
 // the Einstein-Boltzmann power spectrum (compute_power_spectrum), the alternative to power.init
 void create_zero_order_universe(zero_order_universe*, std::function<double(double)>, double, cosmic_params) {
@@ -193,7 +244,53 @@ int DBClose(DBfile*) {
 	abort();
 }
 
+static int power_main(int argc, char** argv) {
+	if (argc != 7) {
+		fprintf(stderr, "usage: ic_probe power N fold box_mpc particles.bin out.bin\n");
+		return 2;
+	}
+	const int N = atoi(argv[2]);
+	const int fold = atoi(argv[3]);
+	ref_set_defaults();
+	FILE* fp = fopen(argv[5], "rb");
+	int64_t n = 0;
+	if (!fp || fread(&n, sizeof(n), 1, fp) != 1) {
+		return 2;
+	}
+	// the binning reads the grid size from parts_dim (src/fft.cpp:245,315), the transform from Nfour
+	g_opts.Nfour = N;
+	g_opts.parts_dim = N;
+	g_opts.nparts = n;
+	g_opts.code_to_cm = atof(argv[4]) * constants::mpc_to_cm;
+	particles_resize(n);
+	for (int d = 0; d < NDIM; d++) {
+		std::vector<uint32_t> x(n);
+		if (fread(x.data(), sizeof(uint32_t), n, fp) != (size_t) n) {
+			return 2;
+		}
+		for (int64_t i = 0; i < n; i++) {
+			particles_pos(d, i).set_integer(x[i]);
+		}
+	}
+	fclose(fp);
+	const power_spectrum_t ps = power_spectrum_compute(fold);
+	fp = fopen(argv[6], "wb");
+	if (!fp) {
+		return 2;
+	}
+	const int64_t m = ps.P.size();
+	fwrite(&m, sizeof(m), 1, fp);
+	fwrite(ps.k.data(), sizeof(float), m, fp);
+	fwrite(ps.P.data(), sizeof(float), m, fp);
+	fwrite(ps.Perr.data(), sizeof(float), m, fp);
+	fclose(fp);
+	return 0;
+}
+
 int main(int argc, char** argv) {
+	if (argc > 1 && std::string(argv[1]) == "power") {
+		return power_main(argc, argv);
+	}
 	if (argc != 10) {
 		fprintf(stderr, "usage: ic_probe N box_mpc z0 omega_m hubble sigma8 twolpt table.txt out.bin\n");
 		return 2;

@@ -1,4 +1,5 @@
-"""Record the reference's own initial conditions as fixtures (tests/golden/ref_ic.npz).
+"""Record the reference's own initial conditions and power spectra as fixtures
+(tests/golden/ref_ic.npz).
 
 The reference's initialize() (src/initialize.cpp:261-355,436-898: the lattice, the Zel'dovich
 displacements of a Gaussian field drawn with GSL's taus generator per k-space row, and the 2LPT
@@ -7,7 +8,10 @@ factor compiled where they lie by `make -C oracle ic` (oracle/ic_probe.cpp; HPX 
 single-threaded stand-in of oracle/stub/hpx, FFTW's one-line transforms plain discrete Fourier
 sums in double precision stored as floats).  For each case below this script writes the
 power.init table the reference reads, the cosmology, and the reference's particle positions
-(fixed32), velocities and growth factors.
+(fixed32), velocities and growth factors.  The same probe runs the reference's matter power
+spectrum (power_spectrum_compute, src/power.cpp:24-77, binned by src/fft.cpp:172-360, the
+density deposited by the kernel of src/power.cu:31-67 run on the host) on seeded particle sets
+("power/..." entries: the particles, grid, fold and the reference's k, P and error per bin).
 
     python tests/golden/make_ic_golden.py            # writes tests/golden/ref_ic.npz
     python tests/golden/make_ic_golden.py --check    # compares a fresh recording with it
@@ -66,8 +70,42 @@ def run_probe(N, box, z0, omega_m, hubble, sigma8, twolpt, k, P):
     return xyz, v, fac
 
 
+def power_cases():
+    """(name, x (3, n) uint32, N, fold): n >= N^3 particles, so that the reference deposits the
+    density in one box (its sub-box path, for fewer particles than cells per rank, deposits
+    particles of neighbouring boxes too and writes up to one cell below and two above each box's
+    array, src/power.cpp:44-61 with src/power.cu:41-57)."""
+    from cosmictiger_b200 import ics
+
+    rng = np.random.default_rng(5)
+    uni = rng.integers(0, 2 ** 32, (3, 16 ** 3), dtype=np.uint64).astype(np.uint32)
+    cx, cy, cz, _, _ = ics.clustered_box(16, nspheres=20, seed=31)
+    clu = np.stack([cx, cy, cz])
+    return [("uniform16_n16_f1", uni, 16, 1), ("uniform16_n16_f2", uni, 16, 2), ("clustered16_n16_f1", clu, 16, 1), ("clustered16_n8_f2", clu, 8, 2)]
+
+
+POWER_BOX = 100.0  # Mpc; scales k only
+
+
+def run_power(x, N, fold):
+    """The reference's power spectrum of particles x (3, n): k, P, Perr (float32)."""
+    with tempfile.TemporaryDirectory() as tmp:
+        parts, out = os.path.join(tmp, "parts.bin"), os.path.join(tmp, "ps.bin")
+        with open(parts, "wb") as f:
+            f.write(np.int64(x.shape[1]).tobytes())
+            f.write(np.ascontiguousarray(x, np.uint32).tobytes())
+        subprocess.run([PROBE, "power", str(N), str(fold), repr(POWER_BOX), parts, out], cwd=tmp, check=True, stdout=subprocess.DEVNULL)
+        raw = open(out, "rb").read()
+    m = int(np.frombuffer(raw[:8], np.int64)[0])
+    return np.frombuffer(raw[8:8 + 12 * m], np.float32).reshape(3, m).copy()
+
+
 def record():
     d = {}
+    for name, x, N, fold in power_cases():
+        d["power/" + name + "/x"] = x
+        d["power/" + name + "/params"] = np.array([N, fold, POWER_BOX], np.float64)
+        d["power/" + name + "/kpe"] = run_power(x, N, fold)
     for name, N, box, z0, om, hub, s8, twolpt, k, P in cases():
         xyz, v, fac = run_probe(N, box, z0, om, hub, s8, twolpt, k, P)
         d[name + "/params"] = np.array([N, box, z0, om, hub, s8, twolpt], np.float64)

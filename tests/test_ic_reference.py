@@ -1,5 +1,6 @@
-"""The IC generator's oracle against the reference's own initial conditions (CPU; the device
-generator, ct_initialize, is compared with the same oracle in tests/test_gpu_fourier.py).
+"""The IC generator's and the power spectrum's oracle against the reference's own initial
+conditions and power spectra (CPU; the device generator and power spectrum, ct_initialize and
+ct_power_spectrum, are compared with the same oracle in tests/test_gpu_fourier.py).
 
 tests/golden/ref_ic.npz holds the output of the reference's initialize() (src/initialize.cpp:
 261-355,436-898) with its 3-D transform (src/fft.cpp) compiled where they lie
@@ -10,7 +11,9 @@ without the 2LPT correction, for two cosmologies and grids.  The numpy restateme
 reference transforms in single precision and keeps its normalisation and growth factors in
 floats, so positions and velocities carry tolerances written below -- relative to the RMS
 displacement for the whole field, and relative to the RMS of the 2LPT correction alone for the
-difference the correction makes.
+difference the correction makes.  The same file holds the reference's power spectrum
+(src/power.cpp:24-77, src/fft.cpp:172-360, the density kernel of src/power.cu:31-67) of seeded
+Poisson and clustered particle sets at two grids and folds.
 """
 import os
 import subprocess
@@ -87,6 +90,29 @@ def test_oracle_2lpt_correction_equals_reference(fix):
         vr = r1v[d].astype(np.float64) - r0v[d]
         vo = o1[3][:, d] - o0[3][:, d]
         assert np.max(np.abs(vr - vo)) < 3e-4 * np.sqrt(np.mean(vo ** 2)), d
+
+
+def power_names(fix):
+    return sorted({k.split("/")[1] for k in fix.files if k.startswith("power/")})
+
+
+def test_oracle_power_spectrum_equals_reference(fix):
+    """Every bin's k within 1e-6, P and its error within 5e-5 relative (the reference deposits
+    and transforms in single precision; measured: below 1.3e-5), and the same empty bins."""
+    names = power_names(fix)
+    assert len(names) == 4
+    for name in names:
+        x = fix["power/" + name + "/x"]
+        N, fold, box = fix["power/" + name + "/params"]
+        k, P, E = fix["power/" + name + "/kpe"]
+        ok, oP, oE, cnt = F.power_spectrum(x[0], x[1], x[2], int(N), int(fold), float(box))
+        assert len(ok) == len(k), name
+        assert np.max(np.abs(k - ok) / ok) < 1e-6, name
+        assert np.array_equal(P == 0, oP == 0), name
+        nz = oP > 0
+        assert nz.sum() >= 10, name
+        assert np.max(np.abs(P[nz] - oP[nz]) / oP[nz]) < 5e-5, name
+        assert np.max(np.abs(E[nz] - oE[nz]) / oE[nz]) < 5e-5, name
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ic_probe")), reason="reference IC probe not built here")
