@@ -3,7 +3,9 @@
 src/power.cu:32-85, src/fft.cpp:172-360), the checker of the CUDA path (ct_initialize,
 ct_power_spectrum).  Transforms are numpy's FFTs in double precision; the random field uses the
 same per-row generator (GSL's "taus", L'Ecuyer 1996, restated below), so that both sides draw
-the same numbers.  Only tests/ import this module.
+the same numbers.  Pinned against the reference's own initialize() and power_spectrum_compute()
+run on the host (oracle/ic_probe.cpp; fixtures tests/golden/ref_ic.npz, tests/test_ic_reference.py).
+Only tests/ import this module.
 """
 import numpy as np
 
