@@ -94,13 +94,15 @@ def read_checkpoint(path, part_int64=False, groups=False, group_int64=False, tra
 
 def write_checkpoint(path, params, x, y, z, v, rung, rung_begin=0, rung_begins=(), part_int64=False):
     """Write a one-rank checkpoint in the reference's layout.  The domain section describes
-    the single rank owning the unit box and all particles."""
+    the single rank owning the unit box and all particles, as the reference's one-rank domain
+    decomposition leaves it (domains_rebound, src/domain.cpp:211-330: key 1, the unit box, rank
+    0; the split coordinate midx is set only for domains it splits, so it stays 0) -- the file
+    is byte for byte the one the reference's write_checkpoint writes for the same state."""
     n = len(x)
     v = np.ascontiguousarray(v, np.float32).reshape(n, 3)
     dom = np.zeros(1, DOMAIN_ENTRY)
     dom["key"] = 1
     dom["box"]["end"] = 1.0
-    dom["midx"] = 0.5
     loc = np.zeros(1, domain_local_dtype(part_int64))
     loc["box"]["end"] = 1.0
     loc["proc_range"] = (0, 1)

@@ -1,8 +1,9 @@
 // Test infrastructure only (oracle build). A single-threaded stand-in for the parts of HPX
-// that the reference's tree build and particle arrays (src/tree.cpp, src/particles.cpp) use,
+// that the reference's host sources compiled by the probes use (src/tree.cpp, src/particles.cpp,
+// src/driver.cpp, src/initialize.cpp, src/fft.cpp, src/power.cpp, src/domain.cpp),
 // so that those sources compile where they lie and run in one process: every async call runs
 // at once on the calling thread and returns a ready future, actions call their function
-// directly (one locality), locks are std locks.  Used only by oracle/tree_probe.cpp.
+// directly (one locality), locks are std locks.  Used only by the probes in oracle/.
 #pragma once
 #include <algorithm>
 #include <cstring>
@@ -244,6 +245,11 @@ future<void> fill(P, It b, It e, const V& v) {
 template<class P, class It, class C>
 future<void> sort(P, It b, It e, C c) {
 	std::sort(b, e, c);
+	return make_ready_future();
+}
+template<class P, class It>
+future<void> sort(P, It b, It e) {
+	std::sort(b, e);
 	return make_ready_future();
 }
 

@@ -1,7 +1,8 @@
 """The reference's checkpoint layout (write_checkpoint, src/driver.cpp:1143-1173; particles_save,
 src/particles.cpp:1206-1227; domains_save, src/domain.cpp:87-94): struct sizes and offsets,
-byte-level layout of the particle section, round trips, and resuming a hierarchical run from a
-checkpoint on the device."""
+byte-level layout of the particle section, round trips, resuming a hierarchical run from a
+checkpoint on the device, and files written and read by the reference's own code
+(oracle/ckpt_probe.cpp): byte-identical in both directions."""
 import struct
 
 import numpy as np
@@ -33,7 +34,7 @@ def test_particle_section_bytes(tmp_path):
     want = struct.pack("<i", 3) + struct.pack("<3I", 1, 2, 3) + struct.pack("<3I", 4, 5, 6) + struct.pack("<3I", 7, 8, 2 ** 32 - 1)
     want += struct.pack("<9f", *range(9)) + struct.pack("<3b", 0, 2, 1) + struct.pack("<3i", 1, 1, 0)
     assert body[:len(want)] == want
-    # domains: one entry (key 1, unit box, midx 0.5, rank 0) and one domain_local
+    # domains: one entry (key 1, unit box, midx 0, rank 0) and one domain_local
     dom = body[len(want):]
     assert len(dom) == 8 + 72 + 72
     assert struct.unpack("<Q", dom[:8])[0] == 1
@@ -168,3 +169,102 @@ def test_reference_fixtures_equal_their_probes(probe, fixture):
     assert out.returncode == 0
     with open(os.path.join(root, "tests", "golden", fixture), "rb") as f:
         assert out.stdout == f.read()
+
+
+# ---------------------------------------------------------------- against the reference's own writer
+# tests/golden/ref_checkpoint.npz: files the reference's write_checkpoint wrote for one rank
+# (oracle/ckpt_probe.cpp; tests/golden/make_ckpt_golden.py), with the states they came from.
+def _ref_ckpt():
+    import os
+
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_checkpoint.npz"))
+
+
+def _ref_cases():
+    return sorted({k.split("/")[0] for k in _ref_ckpt().files})
+
+
+@pytest.mark.parametrize("name", _ref_cases())
+def test_reference_written_checkpoint_reads_and_rewrites_byte_for_byte(tmp_path, name):
+    """A checkpoint the reference wrote reads back to its state -- driver_params, the particles
+    in the order the reference's rung partition left them (this project's CPU oracle applies the
+    same operations to the same particles and gets the same order, range start and saved
+    starts), the one-rank domain section -- and write_checkpoint of that state gives the
+    reference's file byte for byte."""
+    from tests import oracle_lib
+
+    fx = _ref_ckpt()
+    raw = fx[name + "/file"].tobytes()
+    path = tmp_path / "ref.dat"
+    path.write_bytes(raw)
+    c = ck.read_checkpoint(str(path))
+    assert np.asarray(c["params"], ck.DRIVER_PARAMS).tobytes() == fx[name + "/params"].tobytes()
+    x, y, z = (fx[name + "/x"][k].copy() for k in range(3))
+    v = fx[name + "/v"].copy()
+    r = fx[name + "/rung"].copy()
+    begin, stack = 0, []
+    if len(x):
+        orc = oracle_lib.load()
+        for op in fx[name + "/ops"]:
+            if op == "push":
+                stack.append(begin)
+            elif op == "pop":
+                begin = stack.pop()
+            else:
+                m = int(op)
+                begin = 0 if m == 0 else orc.sort_by_rung(x, y, z, v, r, m, begin)
+    assert np.array_equal(c["x"], x) and np.array_equal(c["y"], y) and np.array_equal(c["z"], z)
+    assert np.array_equal(c["v"], v) and np.array_equal(c["rung"], r)
+    assert c["rung_begin"] == begin and c["rung_begins"] == stack
+    assert len(c["domains"]) == 1 and c["domains"]["key"][0] == 1 and c["domains"]["rank"][0] == 0
+    assert c["domain_local"]["part_range"][0].tolist() == [0, len(x)]
+    out = tmp_path / "ours.dat"
+    ck.write_checkpoint(str(out), c["params"], c["x"], c["y"], c["z"], c["v"], c["rung"], c["rung_begin"], c["rung_begins"])
+    assert out.read_bytes() == raw
+
+
+def _ckpt_probe():
+    import os
+
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ckpt_probe")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/ckpt_probe not built (needs the reference's sources)")
+    return exe
+
+
+def test_reference_reads_and_rewrites_our_checkpoint():
+    """Where the probe is built: the reference's read_checkpoint loads a file this module wrote
+    (a state with a rung ladder) and its write_checkpoint writes the same bytes back."""
+    import importlib.util
+    import os
+
+    _ckpt_probe()
+    spec = importlib.util.spec_from_file_location("make_ckpt_golden", os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "make_ckpt_golden.py"))
+    g = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(g)
+    import tempfile
+
+    rng = np.random.default_rng(11)
+    n = 101
+    x, y, z = (rng.integers(0, 2 ** 32, n, dtype=np.uint64).astype(np.uint32) for _ in range(3))
+    v = rng.standard_normal((n, 3)).astype(np.float32)
+    r = np.sort(rng.integers(0, 4, n)).astype(np.int8)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "ours.dat")
+        ck.write_checkpoint(path, ck.default_params(a=0.25, tau=1.5, iter=g.ITER, step=3), x, y, z, v, r, rung_begin=40, rung_begins=[0, 17])
+        mine = np.fromfile(path, np.uint8)
+    assert np.array_equal(g.resave(mine), mine)
+
+
+def test_checkpoint_fixture_equals_a_fresh_run_of_the_reference():
+    """Where the probe is built, a fresh recording from the reference's code equals the committed
+    fixture (guards the fixture against drift of the generator or the probe)."""
+    import os
+    import subprocess
+    import sys
+
+    _ckpt_probe()
+    here = os.path.dirname(os.path.abspath(__file__))
+    res = subprocess.run([sys.executable, os.path.join(here, "golden", "make_ckpt_golden.py"), "--check"], capture_output=True, text=True,
+                         cwd=os.path.dirname(here))
+    assert res.returncode == 0, res.stdout + res.stderr
