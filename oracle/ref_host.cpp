@@ -35,6 +35,8 @@ const vector<hpx::id_type>& hpx_children() {
 }
 void profiler_enter(const char*) {
 }
+void hpx_yield() {
+}
 void profiler_exit() {
 }
 void stack_trace_activate() {
