@@ -825,8 +825,9 @@ void walk(KickCtx& C, KickAcc& acc, int selfi, const float* Lparent, const uint3
 }
 
 // Work items: the walk above a cut (nodes holding more than max_parts particles that are not
-// leaves) hands each non-empty subtree below it, with its check lists and the expansion of its
-// parent, to a work item -- the split the reference makes between its CPU top and its GPU kernel
+// leaves) hands each subtree below it, with its check lists and the expansion of its parent,
+// to a work item (subtrees without particles too, which the reference hands to nobody,
+// kick.cpp:178-181: they carry no particles and no work) -- the split the reference makes between its CPU top and its GPU kernel
 // (kick.cpp:169-190), with the items ordered by their first particle as the reference's
 // kick_workspace orders them (kick_workspace.cpp:308-310).  The top runs level by level, the
 // nodes of one level on all threads.
@@ -1004,8 +1005,7 @@ struct Plan: PlanBase {
 				if (expanded[i]) {
 					nextl.push_back(std::move(kids[2 * i]));
 					nextl.push_back(std::move(kids[2 * i + 1]));
-				} else if (C.nodes[level[i].self].part_end > C.nodes[level[i].self].part_begin) {
-					// a subtree without particles is handed over to nobody (kick.cpp:178-181)
+				} else {
 					items.push_back(std::move(level[i]));
 				}
 			}
